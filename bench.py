@@ -1,0 +1,448 @@
+"""Benchmark: FastLanes FFOR decode at scale on one B200 (the FFOR bit-unpack
+benchmark configuration): one uint32 column of 2^28 values for every bit
+width 0..32 and one uint64 column of 2^27 values for every bit width 0..64,
+values = per-vector base + uniform [0, 2^w).  A step decodes every column
+once into HBM through the library's C ABI.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--workload ffor|ffor-sum|alp] [--scale S]
+
+Prints one JSON line (rank 0).  value = (compressed bytes read + decoded
+bytes written) / device time, whole job.  Inputs are generated on the
+device, as random packed words (every value uniform in [0, 2^w)), and every
+column's output (1 GiB) is larger than L2, so no flush is needed between
+steps.  Multi-GPU runs are independent replicas (the decode path has no
+exchange step): every rank decodes the full column set on its own GPU."""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from concurrent.futures import ThreadPoolExecutor
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "msc-thesis-project_b200"))
+sys.path.insert(0, str(ROOT / "tests"))
+
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d, "measured"
+    return PEAKS_FALLBACK, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.thread.join(timeout=2)
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            parts = [x.strip() for x in l.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (replicas)
+# ---------------------------------------------------------------------------
+def dist_init():
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+# workload: FFOR at scale
+# ---------------------------------------------------------------------------
+def make_ffor_columns(scale: float, dev):
+    """One u32 column of 2^28 * scale values per width 0..32, one u64 column
+    of 2^27 * scale values per width 0..64; random packed words (so every
+    value is uniform in [0, 2^w)), random bases."""
+    import torch
+    import flsgpu_b200 as F
+    cols = []
+    g = torch.Generator(device=dev)
+    g.manual_seed(1234)
+    for bits, n_values in ((32, int(2 ** 28 * scale)), (64, int(2 ** 27 * scale))):
+        n_values -= n_values % 1024
+        n_vecs = n_values // 1024
+        nl = 1024 // bits
+        for w in range(bits + 1):
+            n_words = n_vecs * w * nl
+            packed = torch.randint(-2 ** 31, 2 ** 31, (max(n_words, 1) * (bits // 32),),
+                                   dtype=torch.int32, device=dev, generator=g)
+            packed = packed.view(torch.int64) if bits == 64 else packed
+            bw = torch.full((n_vecs,), w, dtype=torch.uint8, device=dev)
+            offs = torch.arange(n_vecs, dtype=torch.int64, device=dev) * (w * nl)
+            bases = torch.randint(-2 ** 31, 2 ** 31, (n_vecs * (bits // 32),), dtype=torch.int32,
+                                  device=dev, generator=g)
+            bases = bases.view(torch.int64) if bits == 64 else bases
+            bp = F.BPColumnC(n_values, n_vecs, packed.data_ptr(), bw.data_ptr(), offs.data_ptr())
+            c = F.DeviceColumn("ffor", f"u{bits}", n_values,
+                               F.FFORColumnC(n_values, bp, bases.data_ptr()),
+                               {"packed": packed[:n_words * (bits // 32)] if bits == 32 else packed[:n_words],
+                                "bit_widths": bw, "vector_offsets": offs, "bases": bases,
+                                "_keep": packed}, n_words)
+            cols.append((bits, w, c))
+    return cols
+
+
+def col_bytes(c) -> tuple[int, int]:
+    """(compressed bytes read, decoded bytes written) by one full decode:
+    packed words + base + bit width + vector offset per vector; output."""
+    bits = int(c.dtype[1:])
+    read = c.n_packed * bits // 8 + c.n_vecs * (bits // 8 + 1 + 8)
+    return read, c.n_values * bits // 8
+
+
+def run_ffor(args, rank, world, dev):
+    import torch
+    import flsgpu_b200 as F
+
+    cols = make_ffor_columns(args.scale, dev)
+    out = torch.empty(max(c.n_values for _, _, c in cols) * 8 // 4, dtype=torch.int32, device=dev)
+    total_read = sum(col_bytes(c)[0] for _, _, c in cols)
+    total_write = sum(col_bytes(c)[1] for _, _, c in cols)
+    stream = torch.cuda.current_stream()
+    fsum = args.workload == "ffor-sum"
+    sums = torch.zeros(len(cols), dtype=torch.int64, device=dev)
+
+    def step(events=None):
+        for i, (bits, w, c) in enumerate(cols):
+            if events is not None:
+                events[i][0].record(stream)
+            if fsum:
+                F.sum_(c, out=sums[i:i + 1], stream=stream)
+            else:
+                F.decompress(c, out=out.view(torch.int64 if bits == 64 else torch.int32)[:c.n_values],
+                             stream=stream)
+            if events is not None:
+                events[i][1].record(stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    events = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in cols] for _ in range(args.steps)]
+    launches0 = F.launch_count()
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for s in range(args.steps):
+            step(events[s])
+        t1.record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    launches = F.launch_count() - launches0
+    ms = t0.elapsed_time(t1)
+    ms = max_over_ranks(ms, world)
+    per_col_ms = [[events[s][i][0].elapsed_time(events[s][i][1]) for s in range(args.steps)]
+                  for i in range(len(cols))]
+    read_b = total_read if not fsum else total_read
+    write_b = total_write if not fsum else 8 * len(cols)
+    bytes_step = read_b + write_b
+    gbs = bytes_step * args.steps * world / (ms / 1e3) / 1e9
+    per_width = {"u32": [], "u64": []}
+    for (bits, w, c), t in zip(cols, per_col_ms):
+        r, wr = col_bytes(c)
+        b = r + (wr if not fsum else 8)
+        per_width[f"u{bits}"].append(round(b / (statistics.mean(t) / 1e3) / 1e9, 1))
+    # dominant kernel: the FFOR decode launches (one per column); algorithmic
+    # bytes / mean launch duration, over all columns
+    kern_ms = sum(statistics.mean(t) for t in per_col_ms)
+    achieved = bytes_step / (kern_ms / 1e3) / 1e9
+    return dict(gbs=gbs, ms=ms, bytes_step=bytes_step, read=read_b, write=write_b,
+                per_width=per_width, achieved=achieved, launches=launches, clocks=clk.summary(),
+                uncompressed_gbs=total_write * args.steps * world / (ms / 1e3) / 1e9,
+                n_columns=len(cols))
+
+
+# ---------------------------------------------------------------------------
+# end-to-end through the C ABI with host buffers (bounded sample)
+# ---------------------------------------------------------------------------
+def run_e2e(args, dev):
+    """Per step: pinned host packed words + metadata -> device, decode, decoded
+    values -> pinned host.  Sample: one u32 column of 2^24 values for
+    w in {1, 7, 16, 32} and one u64 column of 2^23 values for w in
+    {1, 20, 40, 64}."""
+    import torch
+    import flsgpu_b200 as F
+    stream = torch.cuda.current_stream()
+    rng = np.random.default_rng(7)
+    jobs = []
+    for bits, n_values, widths in ((32, 2 ** 24, (1, 7, 16, 32)), (64, 2 ** 23, (1, 20, 40, 64))):
+        n_vecs = n_values // 1024
+        nl = 1024 // bits
+        ut = np.uint64 if bits == 64 else np.uint32
+        td = torch.int64 if bits == 64 else torch.int32
+        for w in widths:
+            host = {
+                "packed": torch.from_numpy(rng.integers(0, 2 ** bits, n_vecs * w * nl, dtype=np.uint64)
+                                           .astype(ut).view(np.int64 if bits == 64 else np.int32)).pin_memory(),
+                "bit_widths": torch.full((n_vecs,), w, dtype=torch.uint8).pin_memory(),
+                "vector_offsets": (torch.arange(n_vecs, dtype=torch.int64) * (w * nl)).pin_memory(),
+                "bases": torch.from_numpy(rng.integers(0, 2 ** 30, n_vecs).astype(np.int64 if bits == 64 else np.int32)).pin_memory(),
+            }
+            devb = {k: torch.empty_like(v, device=dev) for k, v in host.items()}
+            out_d = torch.empty(n_values, dtype=td, device=dev)
+            out_h = torch.empty(n_values, dtype=td).pin_memory()
+            bp = F.BPColumnC(n_values, n_vecs, devb["packed"].data_ptr(), devb["bit_widths"].data_ptr(),
+                             devb["vector_offsets"].data_ptr())
+            col = F.DeviceColumn("ffor", f"u{bits}", n_values,
+                                 F.FFORColumnC(n_values, bp, devb["bases"].data_ptr()), devb,
+                                 n_vecs * w * nl)
+            jobs.append((host, devb, out_d, out_h, col))
+
+    def step():
+        for host, devb, out_d, out_h, col in jobs:
+            for k in host:
+                devb[k].copy_(host[k], non_blocking=True)
+            F.decompress(col, out=out_d, stream=stream)
+            out_h.copy_(out_d, non_blocking=True)
+
+    for _ in range(2):
+        step()
+    torch.cuda.synchronize()
+    h2d = sum(sum(v.numel() * v.element_size() for v in h.values()) for h, *_ in jobs)
+    d2h = sum(j[3].numel() * j[3].element_size() for j in jobs)
+    reads = sum(col_bytes(j[4])[0] for j in jobs)
+    writes = sum(col_bytes(j[4])[1] for j in jobs)
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    n = 3
+    t0.record(stream)
+    for _ in range(n):
+        step()
+    t1.record(stream)
+    torch.cuda.synchronize()
+    ms = t0.elapsed_time(t1) / n
+    return {"value": round((reads + writes) / (ms / 1e3) / 1e9, 2), "unit": "GB/s",
+            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+            "sample": "u32 2^24 values x w{1,7,16,32} + u64 2^23 x w{1,20,40,64}, "
+                      "pinned host buffers, copies inside the timed region"}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference's own unffor (oracle/_ref), all host cores
+# ---------------------------------------------------------------------------
+def cpu_reference_ffor(seconds_budget: float = 10.0, threads: int | None = None):
+    from oracle import binding as B
+    r = B.ref()
+    kind = "reference"
+    if r is None:
+        r = B.oracle()
+        kind = "port"
+    threads = threads or os.cpu_count() or 1
+    rng = np.random.default_rng(3)
+    work = []
+    for bits, n_vecs in ((32, 256), (64, 128)):
+        ut = np.uint64 if bits == 64 else np.uint32
+        nl = 1024 // bits
+        for w in range(bits + 1):
+            packed = rng.integers(0, 2 ** bits, max(n_vecs * w * nl, 1), dtype=np.uint64).astype(ut)
+            bw = np.full(n_vecs, w, np.uint8)
+            offs = (np.arange(n_vecs, dtype=np.uint64) * (w * nl)).astype(np.uint64)
+            bases = rng.integers(0, 2 ** 30, n_vecs).astype(ut)
+            out = np.zeros(n_vecs * 1024, ut)
+            work.append((bits, w, packed, bw, offs, bases, out, n_vecs))
+    bytes_one = sum(n * w * (1024 // b) * b // 8 + n * (b // 8 + 9) + n * 1024 * b // 8
+                    for b, w, _, _, _, _, _, n in work)
+
+    def run_one(item, v0, v1):
+        bits, w, packed, bw, offs, bases, out, n = item
+        if kind == "reference":
+            fn = r.ref_decode_ffor_u32 if bits == 32 else r.ref_decode_ffor_u64
+            fn(B.ptr(packed), B.ptr(bw), B.ptr(offs), B.ptr(bases), v0, v1, B.ptr(out))
+        else:
+            fn = r.orc_decode_ffor_u32 if bits == 32 else r.orc_decode_ffor_u64
+            fn(B.ptr(packed), B.ptr(bw), B.ptr(offs + 0), B.ptr(bases), v1 - v0, B.ptr(out))
+
+    def one_pass(pool):
+        futs = []
+        for item in work:
+            n = item[7]
+            chunk = max(1, n // threads)
+            for v0 in range(0, n, chunk):
+                futs.append(pool.submit(run_one, item, v0, min(n, v0 + chunk)))
+        for f in futs:
+            f.result()
+
+    with ThreadPoolExecutor(max_workers=threads) as pool:
+        one_pass(pool)
+        t = time.perf_counter()
+        reps = 0
+        while time.perf_counter() - t < seconds_budget:
+            one_pass(pool)
+            reps += 1
+        el = time.perf_counter() - t
+    return {"value": round(bytes_one * reps / el / 1e9, 3), "unit": "GB/s", "cores": threads,
+            "kind": kind,
+            "sample": f"u32 256 vectors x w0..32 + u64 128 vectors x w0..64, {reps} passes in "
+                      f"{el:.1f} s, fls::unffor per vector (src/fls/unffor.cpp:22901/:23005)"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--workload", choices=["ffor", "ffor-sum"], default="ffor")
+    ap.add_argument("--scale", type=float, default=1.0,
+                    help="fraction of the benchmark column sizes (1.0 = full)")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    config = {"workload": "FFOR bit-unpack at scale: u32 2^28 values x w=0..32 + u64 2^27 "
+                          "values x w=0..64, decode to HBM",
+              "columns": 98, "values_u32_per_column": int(2 ** 28 * args.scale),
+              "values_u64_per_column": int(2 ** 27 * args.scale),
+              "l2": "every column's 1 GiB output exceeds L2; no flush",
+              "parallelism": f"replicas x{args.gpus}"}
+    metric = "FFOR decode GB/s (compressed read + decoded write), 1 B200"
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        res = cpu_reference_ffor(args.cpu_seconds)
+        steps_ms = []
+        line = {"impl": "reference", "metric": metric, "value": res["value"], "unit": "GB/s",
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "u32/u64", "data": "synthetic", "config": config,
+                "cpu_baseline": res,
+                "e2e": {"value": res["value"], "unit": "GB/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import torch
+    rank, world, local = dist_init()
+    dev = torch.device("cuda", torch.cuda.current_device())
+    res = run_ffor(args, rank, world, dev)
+    e2e = None if args.no_e2e else run_e2e(args, dev)
+    pk, pk_kind = peaks()
+    hbm = float(pk["hbm_gbs"])
+    if rank == 0:
+        cpu = cpu_reference_ffor(args.cpu_seconds) if world == 1 else None
+        line = {
+            "metric": metric, "value": round(res["gbs"], 1), "unit": "GB/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(res["ms"] / args.steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32/u64", "data": "synthetic",
+            "config": config,
+            "hbm_fraction": {"of_measured": round(res["gbs"] / world / hbm, 4),
+                             "of_spec_8tbs": round(res["gbs"] / world / 8000.0, 4)},
+            "uncompressed_gbs": round(res["uncompressed_gbs"], 1),
+            "per_width_gbs": res["per_width"],
+            "roofline": {"bound": "hbm", "achieved": round(res["achieved"], 1),
+                         "peak": hbm, "unit": "GB/s", "frac": round(res["achieved"] / hbm, 4),
+                         "peak_kind": pk_kind,
+                         "kernel": "k_column<FFOR, STORE> (flsgpu_decompress_ffor_u32/u64)",
+                         "traffic": None},
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": res["launches"],
+            "clocks": res["clocks"],
+        }
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

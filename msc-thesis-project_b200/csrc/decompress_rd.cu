@@ -1,0 +1,154 @@
+// decompress_rd.cu -- ALP-RD decoding (the reference has CPU code only:
+// rd_encoder::decode, src/alp/rd.hpp:146-172).
+//
+// Per vector, one warp:
+//   1. unpack the u16 FastLanes left-index lanes (thread t holds lanes 2t
+//      and 2t+1 in one 32-bit word per line), look each index up in the
+//      vector's 8-entry dictionary (held one entry per lane, fetched with a
+//      shuffle) and stage the 1024 left parts in shared memory;
+//   2. overwrite the left parts of the exception positions (warp-parallel:
+//      positions of a vector are distinct);
+//   3. unpack the right parts (u64 half-lanes / u32 lanes, FFOR base 0) and
+//      write (left << right_bw) | right as the output bit pattern.
+#include <cstring>
+
+#include "kernels.cuh"
+
+namespace flsb200 {
+
+struct RDParams {
+  size_t n_values, n_vecs;
+  const void *right_packed;
+  const uint8_t *right_bw;
+  const size_t *right_offs;
+  const uint16_t *left_packed;
+  const uint8_t *left_bw;
+  const size_t *left_offs;
+  const uint16_t *dicts;
+  const uint32_t *dict_index;
+  const size_t *exc_offs;
+  const uint16_t *exc;
+  const uint16_t *pos;
+  const uint16_t *counts;
+  uint32_t *d_status;
+  void *out;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_alprd(const RDParams p) {
+  using U = typename UintOf<T>::U;
+  constexpr int MAXW = sizeof(U) * 8;
+  __shared__ uint16_t s_left_all[8][VEC];
+  uint16_t *sl = s_left_all[threadIdx.x >> 5];
+  const int t = threadIdx.x & 31;
+  const size_t gw = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const size_t nw = ((size_t)gridDim.x * blockDim.x) >> 5;
+  U *out_all = reinterpret_cast<U *>(p.out);
+
+  for (size_t vi = gw; vi < p.n_vecs; vi += nw) {
+    const int rbw = p.right_bw[vi], lbw = p.left_bw[vi];
+    if (rbw > MAXW || lbw > 16) {
+      if (t == 0 && p.d_status) atomicOr(p.d_status, FLSGPU_BAD_BIT_WIDTH);
+      continue;
+    }
+    const uint16_t dct = (t < 8) ? p.dicts[8 * (size_t)p.dict_index[vi] + t] : 0;
+    const uint16_t *lin = p.left_packed + p.left_offs[vi];
+    switch_width16(lbw, [&](auto wc) {
+      constexpr int W = decltype(wc)::value;
+      uint32_t wr[W > 0 ? W : 1];
+      load_pair16<W>(lin, t, wr);
+      unpack_pair16<W>(wr, [&](int sub, int k, uint32_t idx) {
+        // indices >= 8 only occur at exception positions (patched below)
+        const uint16_t left = (uint16_t)__shfl_sync(0xffffffffu, (uint32_t)dct, idx < 8 ? idx : 7);
+        sl[(2 * t + sub) + 64 * k] = left;
+      });
+    });
+    __syncwarp();
+    const uint32_t cnt = p.counts[vi];
+    const size_t eo = p.exc_offs[vi];
+    bool bad = false;
+    for (uint32_t i = t; i < cnt; i += 32) {
+      const uint32_t ps = p.pos[eo + i];
+      if (ps < VEC)
+        sl[ps] = p.exc[eo + i];
+      else
+        bad = true;
+    }
+    if (__any_sync(0xffffffffu, bad) && t == 0 && p.d_status)
+      atomicOr(p.d_status, FLSGPU_BAD_EXCEPTION);
+    __syncwarp();
+    const size_t vbase = vi * VEC;
+    const size_t rem = p.n_values - vbase;
+    const int lim = rem < (size_t)VEC ? (int)rem : VEC;
+    U *out = out_all + vbase;
+    const U *rin = reinterpret_cast<const U *>(p.right_packed) + p.right_offs[vi];
+    const XInt<U> ident{0};
+    decode_values<U>(rin, rbw, t, ident, [&](int idx, U r) {
+      const U l = rbw >= MAXW ? U(0) : (U)((U)sl[idx] << rbw);
+      if (idx < lim) out[idx] = l | r;
+    });
+    __syncwarp();
+  }
+}
+
+template <typename T>
+static flsgpu_status decompress_rd(const flsgpu_alprd_column *c, T *d_out,
+                                   const flsgpu_decode_opts *o, flsgpu_stream stream) {
+  flsgpu_status s = check_opts(o);
+  if (s) return s;
+  if (!c) return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "null column");
+  RDParams p{};
+  p.n_values = c->n_values;
+  p.n_vecs = vecs_of(c->n_values);
+  if (p.n_vecs == 0) return FLSGPU_OK;
+  if (!d_out) return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "null output");
+  if (((uintptr_t)d_out % sizeof(T)) != 0)
+    return set_error(FLSGPU_ERR_MISALIGNED, "output not aligned");
+  if (((uintptr_t)c->left.packed_array % 4) != 0)
+    return set_error(FLSGPU_ERR_MISALIGNED, "left parts must be 4-byte aligned");
+  p.right_packed = c->right.packed_array;
+  p.right_bw = c->right.bit_widths;
+  p.right_offs = c->right.vector_offsets;
+  p.left_packed = reinterpret_cast<const uint16_t *>(c->left.packed_array);
+  p.left_bw = c->left.bit_widths;
+  p.left_offs = c->left.vector_offsets;
+  p.dicts = c->dictionaries;
+  p.dict_index = c->dictionary_indices;
+  p.exc_offs = c->exceptions_offsets;
+  p.exc = c->exceptions;
+  p.pos = c->positions;
+  p.counts = c->counts;
+  if (!p.right_bw || !p.right_offs || !p.left_bw || !p.left_offs || !p.dicts || !p.dict_index ||
+      !p.counts || !p.exc_offs)
+    return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "null ALP-RD array");
+  p.d_status = o ? o->d_status : nullptr;
+  p.out = d_out;
+  static int bps = 0;
+  if (bps == 0) {
+    int b = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_alprd<T>, 256, 0);
+    bps = b > 0 ? b : 1;
+  }
+  const unsigned grid = persistent_blocks(p.n_vecs, 8, bps);
+  k_alprd<T><<<grid, 256, 0, (cudaStream_t)stream>>>(p);
+  note_launch();
+  return check_cuda(cudaGetLastError(), "k_alprd launch");
+}
+
+}  // namespace flsb200
+
+using namespace flsb200;
+
+extern "C" {
+
+flsgpu_status flsgpu_decompress_alprd_f32(const flsgpu_alprd_column *c, float *o,
+                                          const flsgpu_decode_opts *op, flsgpu_stream s) {
+  return decompress_rd<float>(c, o, op, s);
+}
+
+flsgpu_status flsgpu_decompress_alprd_f64(const flsgpu_alprd_column *c, double *o,
+                                          const flsgpu_decode_opts *op, flsgpu_stream s) {
+  return decompress_rd<double>(c, o, op, s);
+}
+
+}  // extern "C"

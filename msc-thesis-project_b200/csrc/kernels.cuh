@@ -1,0 +1,708 @@
+#pragma once
+// kernels.cuh -- column kernels: full decompression, decode fused with a sum,
+// magic-value scan, synthetic compute, multi-column scan.
+//
+// Work mapping: one warp decodes one 1024-value vector at a time and walks
+// the column with a grid stride over a persistent grid (a whole number of
+// waves on the SMs).  Thread t owns lane t (32-bit types) or half of lane
+// t % 16 (64-bit types, values 32*(t/16) .. +31), so every warp-wide load of
+// a packed line and every warp-wide store of a decoded row is a contiguous
+// 128-byte segment.  The reference instead maps one thread to one lane and
+// one value per call (src/engine/device-utils.cuh:77-120).
+#include <algorithm>
+
+#include "common.cuh"
+#include "unpack.cuh"
+
+namespace flsb200 {
+
+enum Kind { K_BP = 0, K_FFOR = 1, K_ALP = 2, K_ALPX = 3 };
+enum Sink { S_STORE = 0, S_SUM = 1, S_QUERY = 2, S_COMPUTE = 3, S_ALLEQ = 4 };
+
+template <typename T> struct UintOf;
+template <> struct UintOf<uint32_t> { using U = uint32_t; using I = int32_t; };
+template <> struct UintOf<uint64_t> { using U = uint64_t; using I = int64_t; };
+template <> struct UintOf<float> { using U = uint32_t; using I = int32_t; };
+template <> struct UintOf<double> { using U = uint64_t; using I = int64_t; };
+
+struct ColumnParams {
+  size_t n_values, n_vecs;
+  const void *packed;
+  const uint8_t *bw;
+  const size_t *offs;
+  const void *bases;
+  const void *factors, *fractions;
+  const uint8_t *fac_idx, *exp_idx;
+  const size_t *exc_offs;
+  const void *exc;
+  const uint16_t *pos;
+  const uint16_t *counts;  // ALPColumn
+  const uint16_t *oc;      // ALPExtendedColumn
+  int patch;
+  size_t n_packed;         // 0: unchecked
+};
+
+struct KernelParams {
+  ColumnParams c;
+  uint32_t *d_status;
+  void *out;               // S_STORE
+  uint64_t *sum_u64;       // S_SUM integers
+  double *partials;        // S_SUM float: one per vector
+  uint8_t *found;          // S_QUERY / S_COMPUTE / S_ALLEQ
+  uint64_t magic;          // bit pattern of the query value
+  uint32_t n_rep;          // S_COMPUTE
+  uint64_t runtime_zero;   // S_COMPUTE
+};
+
+// ---- value transforms (functors of the reference) ------------------------
+// BPFunctor / FFORFunctor, src/flsgpu/fls.cuh:16-41.
+template <typename U> struct XInt {
+  U base;
+  __device__ __forceinline__ U operator()(U u) const { return u + base; }
+};
+// ALPFunctor, src/flsgpu/alp.cuh:40-45: (T)(INT_T)((u + base) * factor) * frac
+// with unsigned wraparound; conversion and multiply are single RN ops, so
+// the result is the CPU falp's bit for bit.
+struct XAlpF32 {
+  uint32_t base, fact;
+  float frac;
+  __device__ __forceinline__ float operator()(uint32_t u) const {
+    return __fmul_rn(__int2float_rn((int32_t)((u + base) * fact)), frac);
+  }
+};
+struct XAlpF64 {
+  uint64_t base, fact;
+  double frac;
+  __device__ __forceinline__ double operator()(uint64_t u) const {
+    return __dmul_rn(__ll2double_rn((long long)((u + base) * fact)), frac);
+  }
+};
+
+template <typename T, int KIND> struct XformOf { using type = XInt<typename UintOf<T>::U>; };
+template <int KIND> struct XformOf<float, KIND> { using type = XAlpF32; };
+template <int KIND> struct XformOf<double, KIND> { using type = XAlpF64; };
+
+template <typename T> __device__ __forceinline__ T from_bits(uint64_t b) {
+  if constexpr (sizeof(T) == 4) {
+    const uint32_t x = (uint32_t)b;
+    return *reinterpret_cast<const T *>(&x);
+  } else {
+    return *reinterpret_cast<const T *>(&b);
+  }
+}
+
+__device__ __forceinline__ void flag_status(uint32_t *s, uint32_t f) {
+  if (s) atomicOr(s, f);
+}
+
+// Per-vector metadata, loaded one vector ahead of its use (the loads of
+// vector i + stride are in flight while vector i is decoded).
+template <typename T> struct Meta {
+  using U = typename UintOf<T>::U;
+  size_t off;
+  U base;
+  int w;
+  int fi, ei;
+};
+
+template <typename T, int KIND>
+__device__ __forceinline__ Meta<T> load_meta(const ColumnParams &c, size_t vi) {
+  using U = typename UintOf<T>::U;
+  Meta<T> m;
+  m.w = c.bw[vi];
+  m.off = c.offs[vi];
+  m.base = (KIND == K_BP) ? U(0) : reinterpret_cast<const U *>(c.bases)[vi];
+  if constexpr (std::is_floating_point<T>::value) {
+    m.fi = c.fac_idx[vi];
+    m.ei = c.exp_idx[vi];
+  } else {
+    m.fi = m.ei = 0;
+  }
+  return m;
+}
+
+// Validates metadata and builds the transform; false = skip the vector.
+template <typename T, int KIND>
+__device__ __forceinline__ bool setup_from_meta(const ColumnParams &c, uint32_t *d_status,
+                                                const Meta<T> &m, int lane,
+                                                const typename UintOf<T>::U *&vin, int &w,
+                                                typename XformOf<T, KIND>::type &xf) {
+  using U = typename UintOf<T>::U;
+  constexpr int MAXW = sizeof(U) * 8;
+  w = m.w;
+  uint32_t bad = 0;
+  if (w > MAXW) bad |= FLSGPU_BAD_BIT_WIDTH;
+  if (c.n_packed && (m.off > c.n_packed || (size_t)w * Lanes<U>::N > c.n_packed - m.off))
+    bad |= FLSGPU_BAD_OFFSET;
+  vin = reinterpret_cast<const U *>(c.packed) + m.off;
+  xf.base = m.base;
+  if constexpr (std::is_same<T, float>::value) {
+    if (m.fi > 9 || m.ei > 10) bad |= FLSGPU_BAD_PARAMETER_INDEX;
+    if (!bad) {
+      xf.fact = (uint32_t)(c.factors ? reinterpret_cast<const int32_t *>(c.factors)[m.fi]
+                                     : c_f32_fact[m.fi]);
+      xf.frac = c.fractions ? reinterpret_cast<const float *>(c.fractions)[m.ei] : c_f32_frac[m.ei];
+    }
+  } else if constexpr (std::is_same<T, double>::value) {
+    if (m.fi > 18 || m.ei > 20) bad |= FLSGPU_BAD_PARAMETER_INDEX;
+    if (!bad) {
+      xf.fact = (uint64_t)(c.factors ? reinterpret_cast<const int64_t *>(c.factors)[m.fi]
+                                     : c_f64_fact[m.fi]);
+      xf.frac = c.fractions ? reinterpret_cast<const double *>(c.fractions)[m.ei] : c_f64_frac[m.ei];
+    }
+  }
+  if (bad) {
+    if (lane == 0) flag_status(d_status, bad);
+    return false;
+  }
+  return true;
+}
+
+template <typename T, int KIND>
+__device__ __forceinline__ bool vector_setup(const ColumnParams &c, uint32_t *d_status, size_t vi,
+                                             int lane, const typename UintOf<T>::U *&vin, int &w,
+                                             typename XformOf<T, KIND>::type &xf) {
+  return setup_from_meta<T, KIND>(c, d_status, load_meta<T, KIND>(c, vi), lane, vin, w, xf);
+}
+
+// Asks L2 to fetch the packed lines (w lines of 128 B) of the next vector.
+__device__ __forceinline__ void prefetch_packed(const void *vin, int w, int t) {
+  const char *p = reinterpret_cast<const char *>(vin);
+  for (int j = t; j < w; j += 32) asm volatile("prefetch.global.L2 [%0];" ::"l"(p + 128 * j));
+}
+
+// Decodes the calling thread's 32 values of a vector; put(idx, value) with
+// idx the position inside the vector, called in ascending value order.
+// Kernel variant bits (chosen per type and width by the autotuner):
+constexpr int VAR_PREFETCH = 1;  // metadata one vector ahead + L2 prefetch of packed lines
+constexpr int VAR_STCS = 2;      // streaming (evict-first) output stores
+constexpr int VAR_LD32 = 4;      // 64-bit lanes: 32-bit word loads (fewer live registers)
+constexpr int VAR_MINB2 = 8;     // register cap for two resident blocks per SM
+constexpr int VAR_DEFAULT = VAR_PREFETCH;
+
+template <typename T, int VAR = VAR_DEFAULT, class X, class Put>
+__device__ __forceinline__ void decode_values(const typename UintOf<T>::U *vin, int w, int t,
+                                              const X &xf, Put &&put) {
+  using U = typename UintOf<T>::U;
+  if constexpr (sizeof(U) == 4) {
+    switch_width32(w, [&](auto wc) {
+      constexpr int W = decltype(wc)::value;
+      uint32_t wr[W > 0 ? W : 1];
+      load_lane32<W>(vin, t, wr);
+      unpack_lane32<W>(wr, [&](int k, uint32_t u) { put(t + 32 * k, xf(u)); });
+    });
+  } else {
+    const int lane = t & 15, half = t >> 4;
+    switch_width64(w, [&](auto wc) {
+      constexpr int W = decltype(wc)::value;
+      uint32_t wr[W > 0 ? W : 1];
+      if constexpr ((VAR & VAR_LD32) != 0)
+        load_half64_w32<W>(vin, lane, half, wr);
+      else
+        load_half64<W>(vin, lane, half, wr);
+      unpack_half64<W>(wr, [&](int k, uint64_t u) { put(lane + 16 * (32 * half + k), xf(u)); });
+    });
+  }
+}
+
+// Exceptions of vector vi (decoder::patch_exceptions, src/alp/decoder.hpp:
+// 137-145): count = counts[vi] (ALPColumn) or the u16 sum of the per-lane
+// counts (ALPExtendedColumn, as alp::decode reconstructs it,
+// alp-bindings.cu:238-242).  Positions of a vector are distinct, so the
+// warp writes them in parallel.
+template <typename T, int KIND, class Write>
+__device__ __forceinline__ void patch_vector(const ColumnParams &c, uint32_t *d_status, size_t vi,
+                                             int t, Write &&write) {
+  using U = typename UintOf<T>::U;
+  constexpr int NL = Lanes<U>::N;
+  uint32_t cnt;
+  if constexpr (KIND == K_ALP) {
+    cnt = c.counts[vi];
+  } else {
+    uint32_t lc = (t < NL) ? (uint32_t)(c.oc[vi * NL + t] >> 10) : 0u;
+    cnt = __reduce_add_sync(0xffffffffu, lc) & 0xFFFFu;
+  }
+  const size_t eo = c.exc_offs[vi];
+  const T *exc = reinterpret_cast<const T *>(c.exc);
+  bool bad = false;
+  for (uint32_t i = t; i < cnt; i += 32) {
+    const uint32_t ps = c.pos[eo + i];
+    if (ps < VEC)
+      write(ps, exc[eo + i]);
+    else
+      bad = true;
+  }
+  if (__any_sync(0xffffffffu, bad) && t == 0) flag_status(d_status, FLSGPU_BAD_EXCEPTION);
+}
+
+template <typename T, int T_VAR> __device__ __forceinline__ void store_out(T *p, T v) {
+  if constexpr ((T_VAR & VAR_STCS) != 0)
+    __stcs(p, v);
+  else
+    *p = v;
+}
+
+template <typename T, int KIND, int SINK, int VAR = VAR_DEFAULT>
+__global__ void __launch_bounds__(256, (VAR & VAR_MINB2) ? 2 : 1) k_column(const KernelParams p) {
+  using U = typename UintOf<T>::U;
+  using X = typename XformOf<T, KIND>::type;
+  constexpr bool IS_ALP = (KIND == K_ALP || KIND == K_ALPX);
+  // ALP sums / scans stage the patched vector in shared memory.
+  constexpr bool STAGE = IS_ALP && SINK != S_STORE;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *sbuf = reinterpret_cast<T *>(smem_raw) + (threadIdx.x >> 5) * (STAGE ? VEC : 0);
+
+  const int t = threadIdx.x & 31;
+  const size_t gw = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const size_t nw = ((size_t)gridDim.x * blockDim.x) >> 5;
+  const ColumnParams &c = p.c;
+  const T magic = from_bits<T>(p.magic);
+
+  uint64_t acc_u = 0;
+  bool flag = false;
+
+  Meta<T> meta;
+  if (gw < c.n_vecs) meta = load_meta<T, KIND>(c, gw);
+  for (size_t vi = gw; vi < c.n_vecs; vi += nw) {
+    const U *vin;
+    int w;
+    X xf;
+    const Meta<T> cur = meta;
+    if constexpr ((VAR & VAR_PREFETCH) != 0) {
+      const size_t vn = vi + nw;
+      if (vn < c.n_vecs) {
+        meta = load_meta<T, KIND>(c, vn);
+        if (meta.w <= (int)(sizeof(U) * 8))
+          prefetch_packed(reinterpret_cast<const U *>(c.packed) + meta.off, meta.w, t);
+      }
+    } else if (vi + nw < c.n_vecs) {
+      meta = load_meta<T, KIND>(c, vi + nw);
+    }
+    if (!setup_from_meta<T, KIND>(c, p.d_status, cur, t, vin, w, xf)) continue;
+    const size_t vbase = vi * VEC;
+    const size_t rem = c.n_values - vbase;
+    const int lim = rem < (size_t)VEC ? (int)rem : VEC;
+
+    if constexpr (SINK == S_STORE) {
+      T *out = reinterpret_cast<T *>(p.out) + vbase;
+      if (lim == VEC) {
+        decode_values<T, VAR>(vin, w, t, xf, [&](int idx, T v) { store_out<T, VAR>(out + idx, v); });
+      } else {
+        decode_values<T, VAR>(vin, w, t, xf, [&](int idx, T v) {
+          if (idx < lim) store_out<T, VAR>(out + idx, v);
+        });
+      }
+      if constexpr (IS_ALP) {
+        if (c.patch) {
+          __syncwarp();
+          patch_vector<T, KIND>(c, p.d_status, vi, t, [&](int ps, T e) {
+            if (ps < lim) out[ps] = e;
+          });
+        }
+      }
+    } else if constexpr (STAGE) {
+      decode_values<T>(vin, w, t, xf, [&](int idx, T v) { sbuf[idx] = v; });
+      __syncwarp();
+      if (c.patch) patch_vector<T, KIND>(c, p.d_status, vi, t, [&](int ps, T e) { sbuf[ps] = e; });
+      __syncwarp();
+      if constexpr (SINK == S_SUM) {
+        // fixed tree: per-thread ascending sum, warp butterfly
+        double acc = 0.0;
+        if constexpr (sizeof(T) == 8) {
+          const int lane = t & 15, half = t >> 4;
+#pragma unroll 8
+          for (int k = 0; k < 32; ++k) {
+            const int idx = lane + 16 * (32 * half + k);
+            if (idx < lim) acc = __dadd_rn(acc, (double)sbuf[idx]);
+          }
+        }
+#pragma unroll
+        for (int s = 16; s >= 1; s >>= 1) acc = __dadd_rn(acc, __shfl_xor_sync(0xffffffffu, acc, s));
+        if (t == 0) p.partials[vi] = acc;
+      } else if constexpr (SINK == S_QUERY) {
+        for (int idx = t; idx < lim; idx += 32) flag |= (sbuf[idx] == magic);
+      } else if constexpr (SINK == S_ALLEQ) {
+        bool all = true;
+        constexpr int NL = Lanes<U>::N;
+        if (t < NL)
+          for (int k = 0; k < (int)(sizeof(U) * 8); ++k) {
+            const int idx = t + NL * k;
+            if (idx < lim) all &= (sbuf[idx] == magic);
+          }
+        flag |= (t < NL) && all;
+      }
+      __syncwarp();
+    } else {
+      // register sinks for integer columns
+      if constexpr (SINK == S_SUM) {
+        decode_values<T>(vin, w, t, xf, [&](int idx, T v) {
+          if (idx < lim) acc_u += (uint64_t)v;
+        });
+      } else if constexpr (SINK == S_QUERY) {
+        decode_values<T>(vin, w, t, xf, [&](int idx, T v) { flag |= (idx < lim) && (v == magic); });
+      } else if constexpr (SINK == S_COMPUTE) {
+        const T zero = (T)p.runtime_zero;
+        const uint32_t nrep = p.n_rep;
+        decode_values<T>(vin, w, t, xf, [&](int idx, T v) {
+          // kernels::device::compute_column, src/engine/kernels.cuh:75-84
+          for (uint32_t r = 0; r < nrep; ++r) {
+            v *= (T)3;
+            v <<= 3;
+            v += (T)3;
+            v >>= 3;
+            v &= zero;
+          }
+          flag |= (idx < lim) && (v == (T)1);
+        });
+      } else if constexpr (SINK == S_ALLEQ) {
+        bool all = true;
+        decode_values<T>(vin, w, t, xf, [&](int idx, T v) { all &= (idx >= lim) || (v == magic); });
+        if constexpr (sizeof(U) == 8) all = all && __shfl_xor_sync(0xffffffffu, all, 16);
+        flag |= all;
+      }
+    }
+  }
+
+  if constexpr (SINK == S_SUM && !IS_ALP) {
+#pragma unroll
+    for (int s = 16; s >= 1; s >>= 1) acc_u += __shfl_xor_sync(0xffffffffu, acc_u, s);
+    if (t == 0 && acc_u) atomicAdd(reinterpret_cast<unsigned long long *>(p.sum_u64),
+                                   (unsigned long long)acc_u);
+  }
+  if constexpr (SINK == S_QUERY || SINK == S_COMPUTE || SINK == S_ALLEQ) {
+    if (__any_sync(0xffffffffu, flag) && t == 0) *p.found = 1;
+  }
+}
+
+// Pairwise tree over vector partials (stride doubling, aligned chunks of
+// 2048): dst[b] = tree(src[2048 b .. 2048 b + 2047]).
+static __global__ void __launch_bounds__(1024) k_pairwise_f64(const double *src, size_t n, double *dst) {
+  __shared__ double s[2048];
+  const size_t base = (size_t)blockIdx.x * 2048;
+  const size_t m = std::min<size_t>(2048, n - base);
+  for (int i = threadIdx.x; i < 2048; i += 1024) s[i] = (size_t)i < m ? src[base + i] : 0.0;
+  __syncthreads();
+  for (int st = 1; st < 2048; st <<= 1) {
+    const int i = threadIdx.x * 2 * st;
+    if (i < 2048 && (size_t)(i + st) < m) s[i] = __dadd_rn(s[i], s[i + st]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) dst[blockIdx.x] = s[0];
+}
+
+// ---- host side ------------------------------------------------------------
+template <typename T, int KIND, int SINK> struct Launch {
+  static constexpr bool STAGE = (KIND == K_ALP || KIND == K_ALPX) && SINK != S_STORE;
+  static size_t smem() { return STAGE ? (size_t)8 * VEC * sizeof(T) : 0; }
+  static int blocks_per_sm() {
+    static int bps = 0;
+    if (bps == 0) {
+      auto kern = k_column<T, KIND, SINK>;
+      if (smem() > 48 * 1024)
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem());
+      int b = 0;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, 256, smem());
+      bps = b > 0 ? b : 1;
+    }
+    return bps;
+  }
+  static flsgpu_status run(const KernelParams &p, cudaStream_t s) {
+    if (p.c.n_vecs == 0) return FLSGPU_OK;
+    const unsigned grid = persistent_blocks(p.c.n_vecs, 8, blocks_per_sm());
+    k_column<T, KIND, SINK><<<grid, 256, smem(), s>>>(p);
+    note_launch();
+    return check_cuda(cudaGetLastError(), "k_column launch");
+  }
+};
+
+static inline size_t vecs_of(size_t n_values) { return (n_values + VEC - 1) / VEC; }
+
+static inline bool patch_enabled(const flsgpu_decode_opts *o) {
+  return !o || (o->patcher != FLSGPU_PATCHER_NONE && o->patcher != FLSGPU_PATCHER_DUMMY);
+}
+
+static inline flsgpu_status check_opts(const flsgpu_decode_opts *o) {
+  if (!o) return FLSGPU_OK;
+  if (o->unpacker >= FLSGPU_UNPACKER_COUNT)
+    return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "unknown unpacker %u", o->unpacker);
+  if (o->patcher >= FLSGPU_PATCHER_COUNT)
+    return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "unknown patcher %u", o->patcher);
+  if (o->variant >= FLSGPU_VARIANT_COUNT)
+    return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "unknown variant %u", o->variant);
+  if (o->unpack_n_vectors > 8 || o->unpack_n_values > 32)
+    return set_error(FLSGPU_ERR_UNSUPPORTED, "unpack_n_vectors %u / unpack_n_values %u",
+                     o->unpack_n_vectors, o->unpack_n_values);
+  return FLSGPU_OK;
+}
+
+static inline flsgpu_status fill_bp(ColumnParams &c, const flsgpu_bp_column *bp, size_t n_values) {
+  c.n_values = n_values;
+  c.n_vecs = vecs_of(n_values);
+  c.packed = bp->packed_array;
+  c.bw = bp->bit_widths;
+  c.offs = bp->vector_offsets;
+  if (c.n_vecs && (!c.bw || !c.offs))
+    return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "null bit_widths / vector_offsets");
+  return FLSGPU_OK;
+}
+
+static inline flsgpu_status fill(ColumnParams &c, const flsgpu_bp_column *col, const flsgpu_decode_opts *o) {
+  if (!col) return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "null column");
+  c = ColumnParams{};
+  c.n_packed = o ? o->n_packed_values : 0;
+  return fill_bp(c, col, col->n_values);
+}
+static inline flsgpu_status fill(ColumnParams &c, const flsgpu_ffor_column *col, const flsgpu_decode_opts *o) {
+  if (!col) return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "null column");
+  c = ColumnParams{};
+  c.n_packed = o ? o->n_packed_values : 0;
+  flsgpu_status s = fill_bp(c, &col->bp, col->n_values);
+  if (s) return s;
+  c.bases = col->bases;
+  if (c.n_vecs && !c.bases) return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "null bases");
+  return FLSGPU_OK;
+}
+template <typename AC>
+static flsgpu_status fill_alp(ColumnParams &c, const AC *col, const flsgpu_decode_opts *o) {
+  if (!col) return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "null column");
+  flsgpu_status s = fill(c, &col->ffor, o);
+  if (s) return s;
+  c.n_values = col->n_values;
+  c.n_vecs = vecs_of(col->n_values);
+  c.factors = col->factors;
+  c.fractions = col->fractions;
+  c.fac_idx = col->factor_indices;
+  c.exp_idx = col->fraction_indices;
+  c.exc_offs = col->exceptions_offsets;
+  c.exc = col->exceptions;
+  c.pos = col->positions;
+  c.patch = patch_enabled(o) ? 1 : 0;
+  if (c.n_vecs && (!c.fac_idx || !c.exp_idx))
+    return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "null factor / fraction indices");
+  return FLSGPU_OK;
+}
+static inline flsgpu_status fill(ColumnParams &c, const flsgpu_alp_column *col, const flsgpu_decode_opts *o) {
+  flsgpu_status s = fill_alp(c, col, o);
+  if (s) return s;
+  c.counts = col->counts;
+  if (c.patch && c.n_vecs && (!c.counts || !c.exc_offs))
+    return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "null exception arrays");
+  return FLSGPU_OK;
+}
+static inline flsgpu_status fill(ColumnParams &c, const flsgpu_alpx_column *col, const flsgpu_decode_opts *o) {
+  flsgpu_status s = fill_alp(c, col, o);
+  if (s) return s;
+  c.oc = col->offsets_counts;
+  if (c.patch && c.n_vecs && (!c.oc || !c.exc_offs))
+    return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "null exception arrays");
+  return FLSGPU_OK;
+}
+
+template <typename T> static bool aligned(const void *p) {
+  return ((uintptr_t)p % sizeof(T)) == 0;
+}
+
+template <typename T, int KIND, typename Col>
+static flsgpu_status decompress(const Col *col, T *d_out, const flsgpu_decode_opts *o,
+                                flsgpu_stream stream) {
+  flsgpu_status s = check_opts(o);
+  if (s) return s;
+  KernelParams p{};
+  if ((s = fill(p.c, col, o))) return s;
+  if (p.c.n_vecs == 0) return FLSGPU_OK;
+  if (!d_out) return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "null output");
+  if (!aligned<T>(d_out)) return set_error(FLSGPU_ERR_MISALIGNED, "output not aligned");
+  p.d_status = o ? o->d_status : nullptr;
+  p.out = d_out;
+  return Launch<T, KIND, S_STORE>::run(p, (cudaStream_t)stream);
+}
+
+template <typename T, int KIND, typename Col>
+static flsgpu_status query(const Col *col, T magic, uint8_t *d_found, const flsgpu_decode_opts *o,
+                           flsgpu_stream stream) {
+  flsgpu_status s = check_opts(o);
+  if (s) return s;
+  KernelParams p{};
+  if ((s = fill(p.c, col, o))) return s;
+  if (!d_found) return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "null result");
+  p.d_status = o ? o->d_status : nullptr;
+  p.found = d_found;
+  uint64_t bits = 0;
+  memcpy(&bits, &magic, sizeof(T));
+  p.magic = bits;
+  return Launch<T, KIND, S_QUERY>::run(p, (cudaStream_t)stream);
+}
+
+template <typename T, typename Col>
+static flsgpu_status sum_int(const Col *col, uint64_t *d_sum, const flsgpu_decode_opts *o,
+                             flsgpu_stream stream) {
+  flsgpu_status s = check_opts(o);
+  if (s) return s;
+  KernelParams p{};
+  if ((s = fill(p.c, col, o))) return s;
+  if (!d_sum) return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "null sum");
+  if ((s = check_cuda(cudaMemsetAsync(d_sum, 0, sizeof(uint64_t), (cudaStream_t)stream),
+                      "memset sum")))
+    return s;
+  p.d_status = o ? o->d_status : nullptr;
+  p.sum_u64 = d_sum;
+  return Launch<T, K_FFOR, S_SUM>::run(p, (cudaStream_t)stream);
+}
+
+// Reduces n partials (fixed pairwise tree) into *d_sum, using `tmp` (at
+// least (n + 2047) / 2048 elements) as scratch.
+static inline flsgpu_status pairwise_f64(double *partials, size_t n, double *tmp, double *d_sum,
+                                  cudaStream_t stream) {
+  if (n == 0) return check_cuda(cudaMemsetAsync(d_sum, 0, sizeof(double), stream), "memset");
+  double *src = partials, *dst = tmp;
+  while (n > 1) {
+    const size_t nb = (n + 2047) / 2048;
+    double *d = (nb == 1) ? d_sum : dst;
+    k_pairwise_f64<<<(unsigned)nb, 1024, 0, stream>>>(src, n, d);
+    note_launch();
+    flsgpu_status s = check_cuda(cudaGetLastError(), "k_pairwise_f64");
+    if (s) return s;
+    if (nb == 1) return FLSGPU_OK;
+    // ping-pong between the scratch area and the head of the partials
+    double *nsrc = d;
+    dst = (d == tmp) ? partials : tmp;
+    src = nsrc;
+    n = nb;
+  }
+  return check_cuda(cudaMemcpyAsync(d_sum, src, sizeof(double), cudaMemcpyDeviceToDevice, stream),
+                    "copy sum");
+}
+
+template <int KIND, typename Col>
+static flsgpu_status sum_f64(const Col *col, double *d_sum, double *d_partials,
+                             const flsgpu_decode_opts *o, flsgpu_stream stream) {
+  flsgpu_status s = check_opts(o);
+  if (s) return s;
+  KernelParams p{};
+  if ((s = fill(p.c, col, o))) return s;
+  if (!d_sum || (p.c.n_vecs && !d_partials))
+    return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "null sum / partials");
+  p.d_status = o ? o->d_status : nullptr;
+  p.partials = d_partials;
+  if ((s = Launch<double, KIND, S_SUM>::run(p, (cudaStream_t)stream))) return s;
+  return pairwise_f64(d_partials, p.c.n_vecs, d_partials + p.c.n_vecs, d_sum,
+                      (cudaStream_t)stream);
+}
+
+// ---- multi-column conjunctive scan ----------------------------------------
+struct MultiParams {
+  ColumnParams c[16];
+  uint32_t n_cols;
+  uint64_t value;
+  uint8_t *out;
+  uint32_t *d_status;
+};
+
+// multi_column::query_multi_column (src/generated-bindings/
+// multi-column-device-kernels.cuh:11-439): a thread keeps
+// all_columns_equal &= (reg[c] == reg[c-1]) and reg[0] == value over its
+// lane in every column, which is "every value of the lane equals value in
+// every column"; *out = 1 when some lane of some vector satisfies it.
+template <typename T, int KIND>
+__global__ void __launch_bounds__(256) k_multi(const MultiParams mp) {
+  using U = typename UintOf<T>::U;
+  using X = typename XformOf<T, KIND>::type;
+  constexpr bool IS_ALP = (KIND == K_ALP || KIND == K_ALPX);
+  constexpr int NL = Lanes<U>::N;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *sbuf = reinterpret_cast<T *>(smem_raw) + (threadIdx.x >> 5) * (IS_ALP ? VEC : 0);
+  const int t = threadIdx.x & 31;
+  const size_t gw = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const size_t nw = ((size_t)gridDim.x * blockDim.x) >> 5;
+  const T value = from_bits<T>(mp.value);
+  const size_t n_vecs = mp.c[0].n_vecs;
+  bool flag = false;
+  for (size_t vi = gw; vi < n_vecs; vi += nw) {
+    bool all = true;
+    for (uint32_t ci = 0; ci < mp.n_cols; ++ci) {
+      const ColumnParams &c = mp.c[ci];
+      const U *vin;
+      int w;
+      X xf;
+      if (!vector_setup<T, KIND>(c, mp.d_status, vi, t, vin, w, xf)) {
+        all = false;
+        continue;
+      }
+      const size_t rem = c.n_values - vi * VEC;
+      const int lim = rem < (size_t)VEC ? (int)rem : VEC;
+      if constexpr (IS_ALP) {
+        decode_values<T>(vin, w, t, xf, [&](int idx, T v) { sbuf[idx] = v; });
+        __syncwarp();
+        if (c.patch) patch_vector<T, KIND>(c, mp.d_status, vi, t, [&](int ps, T e) { sbuf[ps] = e; });
+        __syncwarp();
+        if (t < NL)
+          for (int k = 0; k < (int)(sizeof(U) * 8); ++k) {
+            const int idx = t + NL * k;
+            all &= (idx >= lim) || (sbuf[idx] == value);
+          }
+        __syncwarp();
+      } else {
+        decode_values<T>(vin, w, t, xf, [&](int idx, T v) { all &= (idx >= lim) || (v == value); });
+      }
+    }
+    if constexpr (IS_ALP) {
+      flag |= (t < NL) && all;
+    } else {
+      if constexpr (sizeof(U) == 8) all = all && __shfl_xor_sync(0xffffffffu, all, 16);
+      flag |= all;
+    }
+  }
+  if (__any_sync(0xffffffffu, flag) && t == 0) *mp.out = 1;
+}
+
+template <typename T, int KIND, typename Col>
+static flsgpu_status multi(const Col *cols, uint32_t n, T value, uint8_t *d_out,
+                           const flsgpu_decode_opts *o, flsgpu_stream stream) {
+  flsgpu_status s = check_opts(o);
+  if (s) return s;
+  if (!cols || n == 0 || n > 16 || !d_out)
+    return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "bad multi-column arguments (n=%u)", n);
+  MultiParams mp{};
+  for (uint32_t i = 0; i < n; ++i) {
+    if ((s = fill(mp.c[i], &cols[i], o))) return s;
+    if (mp.c[i].n_vecs != mp.c[0].n_vecs)
+      return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "columns differ in length");
+  }
+  if (mp.c[0].n_vecs == 0) return FLSGPU_OK;
+  mp.n_cols = n;
+  memcpy(&mp.value, &value, sizeof(T));
+  mp.out = d_out;
+  mp.d_status = o ? o->d_status : nullptr;
+  constexpr bool IS_ALP = (KIND == K_ALP || KIND == K_ALPX);
+  const size_t smem = IS_ALP ? (size_t)8 * VEC * sizeof(T) : 0;
+  static int bps = 0;
+  auto kern = k_multi<T, KIND>;
+  if (bps == 0) {
+    if (smem > 48 * 1024)
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int b = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, 256, smem);
+    bps = b > 0 ? b : 1;
+  }
+  const unsigned grid = persistent_blocks(mp.c[0].n_vecs, 8, bps);
+  kern<<<grid, 256, smem, (cudaStream_t)stream>>>(mp);
+  note_launch();
+  return check_cuda(cudaGetLastError(), "k_multi launch");
+}
+
+template <typename T, typename Col>
+static flsgpu_status compute(const Col *col, uint32_t n_rep, uint8_t *d_out,
+                             const flsgpu_decode_opts *o, flsgpu_stream stream) {
+  flsgpu_status s = check_opts(o);
+  if (s) return s;
+  KernelParams p{};
+  if ((s = fill(p.c, col, o))) return s;
+  if (!d_out) return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "null result");
+  p.d_status = o ? o->d_status : nullptr;
+  p.found = d_out;
+  p.n_rep = n_rep;
+  p.runtime_zero = 0;
+  return Launch<T, K_FFOR, S_COMPUTE>::run(p, (cudaStream_t)stream);
+}
+
+}  // namespace flsb200

@@ -1,0 +1,152 @@
+"""GPU parity of the BP / FFOR kernels against the oracle (bit-exact), on
+the reference's test shapes: every bit width of u32 and u64, mixed widths
+per vector, ragged tails, the FFOR-small benchmark column, fused sums,
+magic-value scans, the synthetic compute kernel and the multi-column scan
+(reference test-fls.sh / test-multi-column.sh sweeps)."""
+import numpy as np
+import pytest
+
+import colgen
+import flsgpu_b200 as F
+from oracle import binding as B
+
+pytestmark = pytest.mark.gpu
+
+
+def _col(c, dev, bp=False):
+    return F.make_ffor_column(c["packed"], c["bit_widths"], c["vector_offsets"],
+                              None if bp else c["bases"], c["n_values"], dev)
+
+
+def _host(t, ut):
+    return t.cpu().numpy().view(ut)
+
+
+@pytest.mark.parametrize("bits", [32, 64])
+def test_ffor_every_width(cuda, bits):
+    ut = np.uint64 if bits == 64 else np.uint32
+    for w in range(bits + 1):
+        c = colgen.random_ffor(100 + w + bits, 9, bits, [w])
+        got = _host(F.decompress(_col(c, cuda)), ut)
+        want = B.decode_ffor(c["packed"], c["bit_widths"], c["vector_offsets"], c["bases"], bits)
+        assert np.array_equal(got, want), f"u{bits} w={w}"
+
+
+@pytest.mark.parametrize("bits", [32, 64])
+def test_bp_every_width(cuda, bits):
+    ut = np.uint64 if bits == 64 else np.uint32
+    for w in range(0, bits + 1, 3):
+        c = colgen.random_ffor(300 + w + bits, 5, bits, [w])
+        got = _host(F.decompress(_col(c, cuda, bp=True)), ut)
+        want = B.decode_bp(c["packed"], c["bit_widths"], c["vector_offsets"], bits)
+        assert np.array_equal(got, want), f"u{bits} w={w}"
+
+
+@pytest.mark.parametrize("bits", [32, 64])
+@pytest.mark.parametrize("variant", [F.VARIANT_AUTO, F.VARIANT_DIRECT, F.VARIANT_STAGED])
+def test_ffor_mixed_widths(cuda, bits, variant):
+    ut = np.uint64 if bits == 64 else np.uint32
+    c = colgen.random_ffor(7 + bits, 3000, bits, range(bits + 1))
+    got = _host(F.decompress(_col(c, cuda), o=F.opts(variant=variant)), ut)
+    want = B.decode_ffor(c["packed"], c["bit_widths"], c["vector_offsets"], c["bases"], bits)
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("bits", [32, 64])
+@pytest.mark.parametrize("n_values", [1, 1000, 1025, 5 * 1024 - 3])
+def test_ragged_tail_is_not_overwritten(cuda, bits, n_values):
+    import torch
+    ut = np.uint64 if bits == 64 else np.uint32
+    n_vecs = (n_values + 1023) // 1024
+    c = colgen.random_ffor(55, n_vecs, bits, [bits // 3, bits], n_values=n_values)
+    out = torch.full((n_values + 2048,), -1, dtype=torch.int64 if bits == 64 else torch.int32,
+                     device=cuda)
+    F.decompress(_col(c, cuda), out=out[:n_values])
+    got = _host(out, ut)
+    want = B.decode_ffor(c["packed"], c["bit_widths"], c["vector_offsets"], c["bases"], bits)
+    assert np.array_equal(got[:n_values], want[:n_values])
+    assert np.all(got[n_values:] == ut(np.iinfo(ut).max))
+
+
+def test_ffor_small_config_roundtrip(cuda):
+    """2^20 u32 values, 1024 vectors, w = 7: decode equals the input and the
+    oracle's unffor."""
+    vals, c = colgen.ffor_config1(1)
+    assert set(c["bit_widths"].tolist()) == {7}
+    got = _host(F.decompress(_col(c, cuda)), np.uint32)
+    assert np.array_equal(got, vals)
+    assert np.array_equal(got, B.decode_ffor(c["packed"], c["bit_widths"], c["vector_offsets"],
+                                             c["bases"], 32))
+
+
+@pytest.mark.parametrize("bits", [32, 64])
+def test_fused_sum(cuda, bits):
+    c = colgen.random_ffor(900 + bits, 2000, bits, range(bits + 1))
+    want = B.decode_ffor(c["packed"], c["bit_widths"], c["vector_offsets"], c["bases"], bits)
+    s = int(F.sum_(_col(c, cuda)).cpu().numpy().view(np.uint64)[0])
+    ref = int(want.astype(np.uint64).sum(dtype=np.uint64))
+    assert s == ref
+
+
+@pytest.mark.parametrize("bits", [32, 64])
+def test_query_found_and_absent(cuda, bits):
+    ut = np.uint64 if bits == 64 else np.uint32
+    c = colgen.random_ffor(40 + bits, 300, bits, [3, 5], base_max=100)
+    col = _col(c, cuda)
+    vals = B.decode_ffor(c["packed"], c["bit_widths"], c["vector_offsets"], c["bases"], bits)
+    present = int(vals[123457 % vals.size])
+    absent = int(vals.max()) + 1
+    assert int(F.query(col, present).item()) == 1
+    assert int(F.query(col, absent).item()) == 0
+    bp = _col(c, cuda, bp=True)
+    raw = B.decode_bp(c["packed"], c["bit_widths"], c["vector_offsets"], bits)
+    assert int(F.query(bp, int(raw[77])).item()) == 1
+    assert int(F.query(bp, int(raw.max()) + 1).item()) == 0
+
+
+@pytest.mark.parametrize("bits", [32, 64])
+def test_compute_column_never_finds_one(cuda, bits):
+    """compute_column ANDs every value with a runtime zero, so the magic
+    value 1 is never seen (src/engine/kernels.cuh:75-88)."""
+    c = colgen.random_ffor(60 + bits, 64, bits, [4, 9])
+    assert int(F.compute(_col(c, cuda), 10).item()) == 0
+
+
+@pytest.mark.parametrize("bits", [32, 64])
+def test_multi_column(cuda, bits):
+    ut = np.uint64 if bits == 64 else np.uint32
+    n_vecs = 40
+    cols = []
+    for i in range(4):
+        c = colgen.random_ffor(70 + i, n_vecs, bits, [0, 3], base_max=2)
+        c["bit_widths"][:] = np.where(np.arange(n_vecs) % 2 == 0, 3, 0)
+        nl = 1024 // bits
+        c["vector_offsets"][:] = np.concatenate([[0], np.cumsum(c["bit_widths"].astype(np.uint64) * nl)[:-1]])
+        c["packed"] = c["packed"][: int(c["bit_widths"].astype(np.int64).sum()) * nl]
+        c["bases"][:] = 5
+        cols.append(c)
+    # width-0 vectors (odd ones) decode to the base 5 everywhere
+    dcols = [_col(c, cuda) for c in cols]
+    assert int(F.query_multi_column(dcols, 5).item()) == 1
+    assert int(F.query_multi_column(dcols, 6).item()) == 0
+    # the reference's own multi-column test queries the type's max: never found
+    assert int(F.query_multi_column(dcols, int(np.iinfo(ut).max)).item()) == 0
+    # break vector lanes of column 2 at every width-0 vector: no lane qualifies
+    cols[2]["bases"][1::2] = 6
+    dcols[2] = _col(cols[2], cuda)
+    assert int(F.query_multi_column(dcols, 5).item()) == 0
+
+
+@pytest.mark.parametrize("bits", [32, 64])
+def test_corrupt_metadata_is_flagged_not_faulted(cuda, bits):
+    import torch
+    c = colgen.random_ffor(11, 16, bits, [5])
+    c["bit_widths"][3] = bits + 1
+    status = torch.zeros(1, dtype=torch.int32, device=cuda)
+    F.decompress(_col(c, cuda), o=F.opts(d_status=status))
+    assert int(status.item()) & F.BAD_BIT_WIDTH
+    # a packed-size bound catches offsets that run past the array
+    c = colgen.random_ffor(12, 16, bits, [5])
+    status.zero_()
+    F.decompress(_col(c, cuda), o=F.opts(d_status=status, n_packed_values=c["packed"].size - 1))
+    assert int(status.item()) & F.BAD_OFFSET
