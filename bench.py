@@ -326,7 +326,7 @@ def cpu_reference_ffor(seconds_budget: float = 10.0, threads: int | None = None)
     threads = threads or os.cpu_count() or 1
     rng = np.random.default_rng(3)
     work = []
-    for bits, n_vecs in ((32, 256), (64, 128)):
+    for bits, n_vecs in ((32, 2048), (64, 1024)):
         ut = np.uint64 if bits == 64 else np.uint32
         nl = 1024 // bits
         for w in range(bits + 1):
@@ -368,14 +368,14 @@ def cpu_reference_ffor(seconds_budget: float = 10.0, threads: int | None = None)
         el = time.perf_counter() - t
     return {"value": round(bytes_one * reps / el / 1e9, 3), "unit": "GB/s", "cores": threads,
             "kind": kind,
-            "sample": f"u32 256 vectors x w0..32 + u64 128 vectors x w0..64, {reps} passes in "
+            "sample": f"u32 2048 vectors x w0..32 + u64 1024 vectors x w0..64, {reps} passes in "
                       f"{el:.1f} s, fls::unffor per vector (src/fls/unffor.cpp:22901/:23005)"}
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--workload", choices=["ffor", "ffor-sum"], default="ffor")

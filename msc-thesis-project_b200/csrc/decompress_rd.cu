@@ -83,7 +83,7 @@ __global__ void __launch_bounds__(256) k_alprd(const RDParams p) {
     U *out = out_all + vbase;
     const U *rin = reinterpret_cast<const U *>(p.right_packed) + p.right_offs[vi];
     const XInt<U> ident{0};
-    decode_values<U>(rin, rbw, t, ident, [&](int idx, U r) {
+    decode_values<U>(rin, rbw, t, ident, [&](int idx, U r, auto...) {
       const U l = rbw >= MAXW ? U(0) : (U)((U)sl[idx] << rbw);
       if (idx < lim) out[idx] = l | r;
     });

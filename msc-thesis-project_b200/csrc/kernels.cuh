@@ -12,6 +12,7 @@
 #include <algorithm>
 
 #include "common.cuh"
+#include "autotune_table.h"
 #include "unpack.cuh"
 
 namespace flsb200 {
@@ -178,7 +179,40 @@ constexpr int VAR_PREFETCH = 1;  // metadata one vector ahead + L2 prefetch of p
 constexpr int VAR_STCS = 2;      // streaming (evict-first) output stores
 constexpr int VAR_LD32 = 4;      // 64-bit lanes: 32-bit word loads (fewer live registers)
 constexpr int VAR_MINB2 = 8;     // register cap for two resident blocks per SM
-constexpr int VAR_DEFAULT = VAR_PREFETCH;
+constexpr int VAR_CHUNK = 16;    // 64-bit lanes: decode half-lanes in two runs of 16
+constexpr int VAR_AUTO = 32;     // per-width policy from autotune_table.h
+constexpr int VAR_PAIR = 64;     // decode two same-width vectors per warp step (policy bit)
+constexpr int VAR_NOPAIR = 128;  // kernel variant: never pair
+constexpr int VAR_MINB4 = 256;   // kernel variant: 32-bit lanes capped for four blocks per SM
+constexpr int VAR_DEFAULT = VAR_AUTO;
+
+// Policy bits in force for width W under kernel variant VAR.
+template <typename U, int VAR> __host__ __device__ constexpr int policy_of(int W) {
+  if constexpr ((VAR & VAR_AUTO) != 0) {
+    return sizeof(U) == 8 ? tuned::kPolicy64[W] : tuned::kPolicy32[W];
+  } else {
+    return VAR;
+  }
+}
+
+// Widths whose policy asks for an L2 prefetch of the next vector.
+template <typename U, int VAR> __host__ __device__ constexpr unsigned long long prefetch_mask() {
+  unsigned long long m = 0;
+  for (int w = 0; w <= (int)(sizeof(U) * 8) && w < 64; ++w)
+    if (policy_of<U, VAR>(w) & VAR_PREFETCH) m |= 1ull << w;
+  return m;
+}
+
+// Widths decoded two vectors at a time (both vectors' loads in flight before
+// either is unpacked): the low widths, whose code leaves most of the
+// register allocation of the widest cases unused.
+template <typename U, int VAR> __host__ __device__ constexpr unsigned long long pair_mask() {
+  unsigned long long m = 0;
+  if (VAR & VAR_NOPAIR) return 0;
+  for (int w = 0; w <= (int)(sizeof(U) * 8) && w < 64; ++w)
+    if (policy_of<U, VAR>(w) & VAR_PAIR) m |= 1ull << w;
+  return m;
+}
 
 template <typename T, int VAR = VAR_DEFAULT, class X, class Put>
 __device__ __forceinline__ void decode_values(const typename UintOf<T>::U *vin, int w, int t,
@@ -187,20 +221,70 @@ __device__ __forceinline__ void decode_values(const typename UintOf<T>::U *vin, 
   if constexpr (sizeof(U) == 4) {
     switch_width32(w, [&](auto wc) {
       constexpr int W = decltype(wc)::value;
+      constexpr int P = policy_of<U, VAR>(W);
       uint32_t wr[W > 0 ? W : 1];
       load_lane32<W>(vin, t, wr);
-      unpack_lane32<W>(wr, [&](int k, uint32_t u) { put(t + 32 * k, xf(u)); });
+      unpack_lane32<W>(wr, [&](int k, uint32_t u) { put(t + 32 * k, xf(u), IntC<P>{}); });
     });
   } else {
     const int lane = t & 15, half = t >> 4;
     switch_width64(w, [&](auto wc) {
       constexpr int W = decltype(wc)::value;
+      constexpr int P = policy_of<U, VAR>(W);
+      if constexpr ((P & VAR_CHUNK) != 0 && W > 8) {
+        decode_half64_chunked<W>(vin, lane, half, [&](int k, uint64_t u) {
+          put(lane + 16 * (32 * half + k), xf(u), IntC<P>{});
+        });
+        return;
+      }
       uint32_t wr[W > 0 ? W : 1];
-      if constexpr ((VAR & VAR_LD32) != 0)
+      if constexpr ((P & VAR_LD32) != 0)
         load_half64_w32<W>(vin, lane, half, wr);
       else
         load_half64<W>(vin, lane, half, wr);
-      unpack_half64<W>(wr, [&](int k, uint64_t u) { put(lane + 16 * (32 * half + k), xf(u)); });
+      unpack_half64<W>(wr, [&](int k, uint64_t u) {
+        put(lane + 16 * (32 * half + k), xf(u), IntC<P>{});
+      });
+    });
+  }
+}
+
+// Two vectors of the same width W: both vectors' packed words are loaded
+// before either is unpacked.  Only called for widths in pair_mask.
+template <typename T, int VAR, class X, class PutA, class PutB>
+__device__ __forceinline__ void decode_pair(const typename UintOf<T>::U *va,
+                                            const typename UintOf<T>::U *vb, int w, int t,
+                                            const X &xa, const X &xb, PutA &&pa, PutB &&pb) {
+  using U = typename UintOf<T>::U;
+  constexpr unsigned long long PM = pair_mask<U, VAR>();
+  if constexpr (sizeof(U) == 4) {
+    switch_width32(w, [&](auto wc) {
+      constexpr int W = decltype(wc)::value;
+      if constexpr (W < 64 && ((PM >> W) & 1)) {
+        constexpr int P = policy_of<U, VAR>(W);
+        uint32_t wa[W > 0 ? W : 1], wb[W > 0 ? W : 1];
+        load_lane32<W>(va, t, wa);
+        load_lane32<W>(vb, t, wb);
+        unpack_lane32<W>(wa, [&](int k, uint32_t u) { pa(t + 32 * k, xa(u), IntC<P>{}); });
+        unpack_lane32<W>(wb, [&](int k, uint32_t u) { pb(t + 32 * k, xb(u), IntC<P>{}); });
+      }
+    });
+  } else {
+    const int lane = t & 15, half = t >> 4;
+    switch_width64(w, [&](auto wc) {
+      constexpr int W = decltype(wc)::value;
+      if constexpr (W < 64 && ((PM >> W) & 1)) {
+        constexpr int P = policy_of<U, VAR>(W);
+        uint32_t wa[W > 0 ? W : 1], wb[W > 0 ? W : 1];
+        load_half64<W>(va, lane, half, wa);
+        load_half64<W>(vb, lane, half, wb);
+        unpack_half64<W>(wa, [&](int k, uint64_t u) {
+          pa(lane + 16 * (32 * half + k), xa(u), IntC<P>{});
+        });
+        unpack_half64<W>(wb, [&](int k, uint64_t u) {
+          pb(lane + 16 * (32 * half + k), xb(u), IntC<P>{});
+        });
+      }
     });
   }
 }
@@ -242,8 +326,129 @@ template <typename T, int T_VAR> __device__ __forceinline__ void store_out(T *p,
     *p = v;
 }
 
+// Resident blocks per SM the register allocation must allow: the decode
+// loop is latency-bound at low widths, so occupancy matters more than
+// keeping every packed word of the widest cases in registers.
+template <typename T, int VAR> constexpr int min_blocks() {
+  return (VAR & VAR_MINB4) ? 4 : (VAR & VAR_MINB2) ? 2 : (sizeof(T) == 4 ? 2 : 1);
+}
+
+// Decodes one vector into the output (row order), then patches its
+// exceptions for ALP columns.
+template <typename T, int KIND, int VAR>
+__device__ __forceinline__ void store_one(const KernelParams &p, size_t vi, const Meta<T> &m,
+                                          int t) {
+  using U = typename UintOf<T>::U;
+  using X = typename XformOf<T, KIND>::type;
+  constexpr bool IS_ALP = (KIND == K_ALP || KIND == K_ALPX);
+  const ColumnParams &c = p.c;
+  const U *vin;
+  int w;
+  X xf;
+  if (!setup_from_meta<T, KIND>(c, p.d_status, m, t, vin, w, xf)) return;
+  const size_t vbase = vi * VEC;
+  const size_t rem = c.n_values - vbase;
+  const int lim = rem < (size_t)VEC ? (int)rem : VEC;
+  T *out = reinterpret_cast<T *>(p.out) + vbase;
+  if (lim == VEC) {
+    decode_values<T, VAR>(vin, w, t, xf, [&](int idx, T v, auto pc) {
+      store_out<T, decltype(pc)::value>(out + idx, v);
+    });
+  } else {
+    decode_values<T, VAR>(vin, w, t, xf, [&](int idx, T v, auto pc) {
+      if (idx < lim) store_out<T, decltype(pc)::value>(out + idx, v);
+    });
+  }
+  if constexpr (IS_ALP) {
+    if (c.patch) {
+      __syncwarp();
+      patch_vector<T, KIND>(c, p.d_status, vi, t, [&](int ps, T e) {
+        if (ps < lim) out[ps] = e;
+      });
+    }
+  }
+}
+
+// Full decompression.  The warp walks its vectors with a stride of the
+// grid's warp count, keeping the metadata of the next one or two vectors in
+// flight; two consecutive vectors of the same low width are decoded as a
+// pair (decode_pair).
+template <typename T, int KIND, int VAR = VAR_DEFAULT>
+__global__ void __launch_bounds__(256, min_blocks<T, VAR>()) k_store(const KernelParams p) {
+  using U = typename UintOf<T>::U;
+  using X = typename XformOf<T, KIND>::type;
+  constexpr bool IS_ALP = (KIND == K_ALP || KIND == K_ALPX);
+  constexpr unsigned long long PM = pair_mask<U, VAR>();
+  const int t = threadIdx.x & 31;
+  const size_t gw = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const size_t nw = ((size_t)gridDim.x * blockDim.x) >> 5;
+  const ColumnParams &c = p.c;
+  const size_t n = c.n_vecs;
+  T *const out_all = reinterpret_cast<T *>(p.out);
+  (void)out_all;
+
+  Meta<T> ma, mb;
+  size_t vi = gw;
+  if (vi < n) ma = load_meta<T, KIND>(c, vi);
+  bool hb = vi + nw < n;
+  if (hb) mb = load_meta<T, KIND>(c, vi + nw);
+  while (vi < n) {
+    // pair when both vectors are full and share a width marked for pairing
+    const bool pair = PM != 0 && hb && ma.w == mb.w && ma.w < 64 && ((PM >> ma.w) & 1) &&
+                      (vi + nw) * VEC + VEC <= c.n_values;
+    Meta<T> na, nb;
+    bool hnb;
+    if (pair) {
+      if (vi + 2 * nw < n) na = load_meta<T, KIND>(c, vi + 2 * nw);
+      hnb = vi + 3 * nw < n;
+      if (hnb) nb = load_meta<T, KIND>(c, vi + 3 * nw);
+    } else {
+      na = mb;
+      hnb = vi + 2 * nw < n;
+      if (hnb) nb = load_meta<T, KIND>(c, vi + 2 * nw);
+    }
+    if constexpr ((VAR & VAR_PREFETCH) != 0) {
+      const size_t vn = vi + (pair ? 2 : 1) * nw;
+      if (vn < n && na.w <= (int)(sizeof(U) * 8) && ((prefetch_mask<U, VAR>() >> na.w) & 1))
+        prefetch_packed(reinterpret_cast<const U *>(c.packed) + na.off, na.w, t);
+    }
+    if (pair) {
+      const U *va, *vb;
+      int wa, wb;
+      X xa, xb;
+      const bool oka = setup_from_meta<T, KIND>(c, p.d_status, ma, t, va, wa, xa);
+      const bool okb = setup_from_meta<T, KIND>(c, p.d_status, mb, t, vb, wb, xb);
+      const size_t vj = vi + nw;
+      if (oka && okb) {
+        T *outa = out_all + vi * VEC, *outb = out_all + vj * VEC;
+        decode_pair<T, VAR>(
+            va, vb, wa, t, xa, xb,
+            [&](int idx, T v, auto pc) { store_out<T, decltype(pc)::value>(outa + idx, v); },
+            [&](int idx, T v, auto pc) { store_out<T, decltype(pc)::value>(outb + idx, v); });
+        if constexpr (IS_ALP) {
+          if (c.patch) {
+            __syncwarp();
+            patch_vector<T, KIND>(c, p.d_status, vi, t, [&](int ps, T e) { outa[ps] = e; });
+            patch_vector<T, KIND>(c, p.d_status, vj, t, [&](int ps, T e) { outb[ps] = e; });
+          }
+        }
+      } else {
+        if (oka) store_one<T, KIND, VAR>(p, vi, ma, t);
+        if (okb) store_one<T, KIND, VAR>(p, vj, mb, t);
+      }
+      vi += 2 * nw;
+    } else {
+      store_one<T, KIND, VAR>(p, vi, ma, t);
+      vi += nw;
+    }
+    ma = na;
+    mb = nb;
+    hb = hnb;
+  }
+}
+
 template <typename T, int KIND, int SINK, int VAR = VAR_DEFAULT>
-__global__ void __launch_bounds__(256, (VAR & VAR_MINB2) ? 2 : 1) k_column(const KernelParams p) {
+__global__ void __launch_bounds__(256, min_blocks<T, VAR>()) k_column(const KernelParams p) {
   using U = typename UintOf<T>::U;
   using X = typename XformOf<T, KIND>::type;
   constexpr bool IS_ALP = (KIND == K_ALP || KIND == K_ALPX);
@@ -272,7 +477,7 @@ __global__ void __launch_bounds__(256, (VAR & VAR_MINB2) ? 2 : 1) k_column(const
       const size_t vn = vi + nw;
       if (vn < c.n_vecs) {
         meta = load_meta<T, KIND>(c, vn);
-        if (meta.w <= (int)(sizeof(U) * 8))
+        if (meta.w <= (int)(sizeof(U) * 8) && (prefetch_mask<U, VAR>() >> meta.w) & 1)
           prefetch_packed(reinterpret_cast<const U *>(c.packed) + meta.off, meta.w, t);
       }
     } else if (vi + nw < c.n_vecs) {
@@ -286,10 +491,12 @@ __global__ void __launch_bounds__(256, (VAR & VAR_MINB2) ? 2 : 1) k_column(const
     if constexpr (SINK == S_STORE) {
       T *out = reinterpret_cast<T *>(p.out) + vbase;
       if (lim == VEC) {
-        decode_values<T, VAR>(vin, w, t, xf, [&](int idx, T v) { store_out<T, VAR>(out + idx, v); });
+        decode_values<T, VAR>(vin, w, t, xf, [&](int idx, T v, auto pc) {
+          store_out<T, decltype(pc)::value>(out + idx, v);
+        });
       } else {
-        decode_values<T, VAR>(vin, w, t, xf, [&](int idx, T v) {
-          if (idx < lim) store_out<T, VAR>(out + idx, v);
+        decode_values<T, VAR>(vin, w, t, xf, [&](int idx, T v, auto pc) {
+          if (idx < lim) store_out<T, decltype(pc)::value>(out + idx, v);
         });
       }
       if constexpr (IS_ALP) {
@@ -301,7 +508,7 @@ __global__ void __launch_bounds__(256, (VAR & VAR_MINB2) ? 2 : 1) k_column(const
         }
       }
     } else if constexpr (STAGE) {
-      decode_values<T>(vin, w, t, xf, [&](int idx, T v) { sbuf[idx] = v; });
+      decode_values<T>(vin, w, t, xf, [&](int idx, T v, auto...) { sbuf[idx] = v; });
       __syncwarp();
       if (c.patch) patch_vector<T, KIND>(c, p.d_status, vi, t, [&](int ps, T e) { sbuf[ps] = e; });
       __syncwarp();
@@ -335,15 +542,15 @@ __global__ void __launch_bounds__(256, (VAR & VAR_MINB2) ? 2 : 1) k_column(const
     } else {
       // register sinks for integer columns
       if constexpr (SINK == S_SUM) {
-        decode_values<T>(vin, w, t, xf, [&](int idx, T v) {
+        decode_values<T>(vin, w, t, xf, [&](int idx, T v, auto...) {
           if (idx < lim) acc_u += (uint64_t)v;
         });
       } else if constexpr (SINK == S_QUERY) {
-        decode_values<T>(vin, w, t, xf, [&](int idx, T v) { flag |= (idx < lim) && (v == magic); });
+        decode_values<T>(vin, w, t, xf, [&](int idx, T v, auto...) { flag |= (idx < lim) && (v == magic); });
       } else if constexpr (SINK == S_COMPUTE) {
         const T zero = (T)p.runtime_zero;
         const uint32_t nrep = p.n_rep;
-        decode_values<T>(vin, w, t, xf, [&](int idx, T v) {
+        decode_values<T>(vin, w, t, xf, [&](int idx, T v, auto...) {
           // kernels::device::compute_column, src/engine/kernels.cuh:75-84
           for (uint32_t r = 0; r < nrep; ++r) {
             v *= (T)3;
@@ -356,7 +563,7 @@ __global__ void __launch_bounds__(256, (VAR & VAR_MINB2) ? 2 : 1) k_column(const
         });
       } else if constexpr (SINK == S_ALLEQ) {
         bool all = true;
-        decode_values<T>(vin, w, t, xf, [&](int idx, T v) { all &= (idx >= lim) || (v == magic); });
+        decode_values<T>(vin, w, t, xf, [&](int idx, T v, auto...) { all &= (idx >= lim) || (v == magic); });
         if constexpr (sizeof(U) == 8) all = all && __shfl_xor_sync(0xffffffffu, all, 16);
         flag |= all;
       }
@@ -394,10 +601,16 @@ static __global__ void __launch_bounds__(1024) k_pairwise_f64(const double *src,
 template <typename T, int KIND, int SINK> struct Launch {
   static constexpr bool STAGE = (KIND == K_ALP || KIND == K_ALPX) && SINK != S_STORE;
   static size_t smem() { return STAGE ? (size_t)8 * VEC * sizeof(T) : 0; }
+  static auto kernel() {
+    if constexpr (SINK == S_STORE)
+      return k_store<T, KIND>;
+    else
+      return k_column<T, KIND, SINK>;
+  }
   static int blocks_per_sm() {
     static int bps = 0;
     if (bps == 0) {
-      auto kern = k_column<T, KIND, SINK>;
+      auto kern = kernel();
       if (smem() > 48 * 1024)
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem());
       int b = 0;
@@ -409,7 +622,7 @@ template <typename T, int KIND, int SINK> struct Launch {
   static flsgpu_status run(const KernelParams &p, cudaStream_t s) {
     if (p.c.n_vecs == 0) return FLSGPU_OK;
     const unsigned grid = persistent_blocks(p.c.n_vecs, 8, blocks_per_sm());
-    k_column<T, KIND, SINK><<<grid, 256, smem(), s>>>(p);
+    kernel()<<<grid, 256, smem(), s>>>(p);
     note_launch();
     return check_cuda(cudaGetLastError(), "k_column launch");
   }
@@ -631,7 +844,7 @@ __global__ void __launch_bounds__(256) k_multi(const MultiParams mp) {
       const size_t rem = c.n_values - vi * VEC;
       const int lim = rem < (size_t)VEC ? (int)rem : VEC;
       if constexpr (IS_ALP) {
-        decode_values<T>(vin, w, t, xf, [&](int idx, T v) { sbuf[idx] = v; });
+        decode_values<T>(vin, w, t, xf, [&](int idx, T v, auto...) { sbuf[idx] = v; });
         __syncwarp();
         if (c.patch) patch_vector<T, KIND>(c, mp.d_status, vi, t, [&](int ps, T e) { sbuf[ps] = e; });
         __syncwarp();
@@ -642,7 +855,7 @@ __global__ void __launch_bounds__(256) k_multi(const MultiParams mp) {
           }
         __syncwarp();
       } else {
-        decode_values<T>(vin, w, t, xf, [&](int idx, T v) { all &= (idx >= lim) || (v == value); });
+        decode_values<T>(vin, w, t, xf, [&](int idx, T v, auto...) { all &= (idx >= lim) || (v == value); });
       }
     }
     if constexpr (IS_ALP) {

@@ -99,6 +99,62 @@ __device__ __forceinline__ void unpack_half64(const uint32_t *w, F &&f) {
   }
 }
 
+// Chunked form for wide values: the half-lane's 32 values are decoded as
+// two runs of 16, each loading only the 64-bit lines it spans, with a
+// compiler barrier between the runs so that at most ~W/2 + 2 packed words
+// are live.  This lowers register pressure (and raises occupancy) at the
+// price of exposing the second run's load latency to the warp.
+template <int W, class F>
+__device__ __forceinline__ void decode_half64_chunked(const uint64_t *vin, int lane, int half,
+                                                      F &&f) {
+  const int m0 = half * W;
+  const bool odd = (m0 & 1) != 0;
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+    // stream words [J0, J1] (relative to the half) hold values 16c .. 16c+15
+    constexpr int CW = (W > 0) ? W : 1;
+    const int J0 = (16 * c * W) >> 5;
+    const int J1 = (16 * (c + 1) * W + 31) >> 5;  // one past the last word
+    constexpr int NMAX = (16 * CW + 31) / 32 + 2;
+    uint32_t w[NMAX];
+    // 64-bit lines covering stream words m0+J0 .. m0+J1-1
+    const int l0 = (m0 + J0) >> 1;
+    uint64_t d[NMAX / 2 + 2];
+#pragma unroll
+    for (int i = 0; i < NMAX / 2 + 2; ++i) {
+      const int j = l0 + i;
+      const bool need = (2 * i) < (J1 - J0 + 2);
+      d[i] = (need && j < W) ? ld_stream_u64(vin + j * 16 + lane) : 0ull;
+    }
+    // word J0 + i is 64-bit line l0 + ((s + i) >> 1), half (s + i) & 1,
+    // where s = (m0 + J0) & 1 (odd iff half * W + J0 is odd)
+    const bool s = (((J0 & 1) != 0) != odd);
+#pragma unroll
+    for (int i = 0; i < NMAX; ++i) {
+      const uint32_t ev = (i & 1) ? (uint32_t)(d[i >> 1] >> 32) : (uint32_t)d[i >> 1];
+      const uint32_t od = (i & 1) ? (uint32_t)d[(i + 1) >> 1] : (uint32_t)(d[i >> 1] >> 32);
+      w[i] = s ? od : ev;
+    }
+#pragma unroll
+    for (int k = 16 * c; k < 16 * c + 16; ++k) {
+      uint64_t v = 0;
+      if (W > 0) {
+        const int bit = k * W, j = (bit >> 5) - J0, o = bit & 31;
+        const int je = ((bit + W - 1) >> 5) - J0;
+        const uint32_t x0 = w[j];
+        const uint32_t x1 = (je >= j + 1) ? w[j + 1] : 0u;
+        const uint32_t x2 = (je >= j + 2) ? w[j + 2] : 0u;
+        const uint32_t lo = o ? funnel_r(x0, x1, (uint32_t)o) : x0;
+        uint32_t hi = 0;
+        if (W > 32 - o) hi = o ? funnel_r(x1, x2, (uint32_t)o) : x1;
+        v = (((uint64_t)hi << 32) | lo) & mask64<W>();
+      }
+      f(k, v);
+    }
+    asm volatile("" ::: "memory");
+  }
+}
+
 // ---- 16-bit lanes (ALP-RD left indices): one thread per lane pair -------
 // 32-bit word j*32 + t holds 16-bit line j of lanes 2t (low) and 2t+1.
 // Each 16-bit lane has 16 values; f(sub, k, v) receives lane 2t+sub.
