@@ -217,6 +217,22 @@ flsgpu_status flsgpu_sum_alpx_f64(const flsgpu_alpx_column *column, double *d_su
                                   double *d_partials, const flsgpu_decode_opts *opts,
                                   flsgpu_stream stream);
 
+/* Decode-and-sum of an f64 ALP column that allocates nothing.  No
+ * counterpart in the reference.  For callers that cannot provide device
+ * memory (an engine with its own fixed memory budget, a thread capturing a
+ * CUDA graph, a plug-in that must not touch the host process's allocator):
+ * the scratch of the fixed reduction tree lives in a static device array of
+ * FLSGPU_NOALLOC_MAX_VECTORS vectors (2 MiB), reserved on every GPU that
+ * loads the library until the process exits.  Same result, bit for bit, as
+ * flsgpu_sum_alp_f64.  Columns of more vectors are rejected with
+ * FLSGPU_ERR_INVALID_ARGUMENT.  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress); make that first call before
+ * any stream capture.  All calls on a device share the array: calls whose
+ * kernels overlap on the GPU race, so serialise them. */
+#define FLSGPU_NOALLOC_MAX_VECTORS 262144
+flsgpu_status flsgpu_sum_alp_f64_noalloc(const flsgpu_alp_column *column, double *d_sum,
+                                         const flsgpu_decode_opts *opts, flsgpu_stream stream);
+
 /* ---- magic-value scan (kernels::device::query_column, kernels.cuh:34-54;
  *      bindings::query_column, kernel-bindings.cuh:92-131).  *d_found is
  *      set to 1 when some decoded value equals `magic` (float compare) and
