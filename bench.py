@@ -249,6 +249,196 @@ def run_ffor(args, rank, world, dev):
 
 
 # ---------------------------------------------------------------------------
+# workload: batched uneven decode + fused pair query
+# ---------------------------------------------------------------------------
+def make_batch_columns(n_cols: int, dev, seed: int = 4):
+    """n_cols columns, lengths log-uniform in 2^10..2^24 rounded up to 1024;
+    types cycle (f64 ALP, u32 FFOR, f32 ALP); each f64 column and the u32
+    column after it share a length and form a query pair (A, B).  Columns
+    are generated at the compressed level, as the reference's own test data
+    (src/engine/data.cuh:354-477): random packed words at a chosen width,
+    FFOR widths uniform 0..32, ALP widths uniform 16..24 (the range that
+    integers up to 10^6 scaled by 10^d encode to), ALP factor / exponent
+    indices in the lower half of their tables, per-column exception rate
+    uniform in [0, 5%] with positions spread over the vector."""
+    import torch
+    import flsgpu_b200 as F
+    rng = np.random.default_rng(seed)
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    cols, pairs = [], []
+    length = 1024
+
+    def rint32(n):
+        return torch.randint(-2 ** 31, 2 ** 31, (max(n, 1),), dtype=torch.int32, device=dev,
+                             generator=g)
+
+    for i in range(n_cols):
+        kind = i % 3
+        if kind != 1:
+            length = int(2 ** rng.uniform(10, 24))
+            length = (length + 1023) // 1024 * 1024
+        n_vecs = length // 1024
+        if kind == 1:  # u32 FFOR
+            w = int(rng.integers(0, 33))
+            packed = rint32(n_vecs * w * 32)
+            bw = torch.full((n_vecs,), w, dtype=torch.uint8, device=dev)
+            offs = torch.arange(n_vecs, dtype=torch.int64, device=dev) * (w * 32)
+            bases = rint32(n_vecs)
+            bp = F.BPColumnC(length, n_vecs, packed.data_ptr(), bw.data_ptr(), offs.data_ptr())
+            c = F.DeviceColumn("ffor", "u32", length, F.FFORColumnC(length, bp, bases.data_ptr()),
+                               {"packed": packed[: n_vecs * w * 32], "bit_widths": bw,
+                                "vector_offsets": offs, "bases": bases, "_keep": packed},
+                               n_vecs * w * 32)
+            pairs.append((cols[-1], c))
+        else:
+            f64 = kind == 0
+            words = 2 if f64 else 1
+            nl = 16 if f64 else 32
+            w = int(rng.integers(16, 25))
+            n_words = n_vecs * w * nl
+            packed = rint32(n_words * words)
+            bw = torch.full((n_vecs,), w, dtype=torch.uint8, device=dev)
+            offs = torch.arange(n_vecs, dtype=torch.int64, device=dev) * (w * nl)
+            bases = torch.randint(2, 21, (n_vecs,), dtype=torch.int64 if f64 else torch.int32,
+                                  device=dev, generator=g)
+            fac = torch.randint(0, 9 if f64 else 5, (n_vecs,), dtype=torch.uint8, device=dev,
+                                generator=g)
+            exp = torch.randint(0, 10 if f64 else 5, (n_vecs,), dtype=torch.uint8, device=dev,
+                                generator=g)
+            rate = float(rng.uniform(0.0, 0.05))
+            cmax = int(round(2 * rate * 1024))
+            counts = torch.randint(0, cmax + 1, (n_vecs,), dtype=torch.int32, device=dev,
+                                   generator=g)
+            eoffs = torch.cumsum(counts.to(torch.int64), 0) - counts.to(torch.int64)
+            n_exc = int(counts.sum().item())
+            step = 1024 // max(cmax, 1)
+            # positions: exception j of vector v at j*step + (v*7 % step), sorted and distinct
+            vec_of = torch.repeat_interleave(torch.arange(n_vecs, device=dev), counts.to(torch.int64))
+            j = torch.arange(n_exc, device=dev) - eoffs[vec_of] if n_exc else torch.zeros(0, device=dev, dtype=torch.int64)
+            pos = (j * step + (vec_of * 7) % step).to(torch.int16) if n_exc else torch.zeros(1, dtype=torch.int16, device=dev)
+            exc = rint32(max(n_exc, 1) * words)
+            exc = exc.view(torch.float64) if f64 else exc.view(torch.float32)
+            fbuf = {"packed": packed[: n_words * words], "bit_widths": bw, "vector_offsets": offs,
+                    "bases": bases, "factor_indices": fac, "fraction_indices": exp,
+                    "exceptions_offsets": eoffs, "exceptions": exc[:n_exc], "positions": pos[:n_exc],
+                    "counts": counts.to(torch.int16), "_keep": (packed, exc, pos)}
+            bp = F.BPColumnC(length, n_vecs, packed.data_ptr(), bw.data_ptr(), offs.data_ptr())
+            ff = F.FFORColumnC(length, bp, bases.data_ptr())
+            ac = F.ALPColumnC(length, ff, None, None, fac.data_ptr(), exp.data_ptr(), n_exc,
+                              eoffs.data_ptr(), exc.data_ptr(), pos.data_ptr(),
+                              fbuf["counts"].data_ptr())
+            c = F.DeviceColumn("alp", "f64" if f64 else "f32", length, ac, fbuf, n_words)
+        cols.append(c)
+    return cols, pairs
+
+
+def run_batch(args, dev):
+    import torch
+    import flsgpu_b200 as F
+    t0 = time.perf_counter()
+    cols, pairs = make_batch_columns(args.columns, dev)
+    outs = [torch.empty(c.n_values, dtype=getattr(torch, F.TORCH_OF_BITS[c.dtype]), device=dev)
+            for c in cols]
+    gen_s = time.perf_counter() - t0
+    b = F.Batch(cols, outs)
+    stream = torch.cuda.current_stream()
+    read_b = sum(c.compressed_bytes() for c in cols)
+    write_b = sum(o.numel() * o.element_size() for o in outs)
+
+    def timed(fn, steps, warm):
+        for _ in range(warm):
+            fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    b.capture(stream)
+    launches0 = F.launch_count()
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        ms_graph = timed(lambda: b.replay(stream), args.steps, args.warmup)
+    launches = (F.launch_count() - launches0) // (args.steps + args.warmup)
+    ms_launch = timed(lambda: b.decompress(stream), args.steps, args.warmup)
+    ms_each = timed(lambda: b.decompress_each(False, stream), max(2, args.steps // 4), 2)
+    ms_each_sync = timed(lambda: b.decompress_each(True, stream), 2, 1)
+    q = F.PairQuery([p[0] for p in pairs], [p[1] for p in pairs], dev)
+    q.capture(stream)
+    ms_query = timed(lambda: q.replay(stream), max(3, args.steps // 2), 3)
+    q_read = sum(a.compressed_bytes() + bb.compressed_bytes() for a, bb in pairs)
+    return dict(ms=ms_graph, ms_launch=ms_launch, ms_each=ms_each, ms_each_sync=ms_each_sync,
+                read=read_b, write=write_b, clocks=clk.summary(), launches=launches,
+                n_values=sum(c.n_values for c in cols), gen_s=gen_s, ms_query=ms_query,
+                q_read=q_read, n_pairs=len(pairs))
+
+
+# ---------------------------------------------------------------------------
+# workload: learned ALP parameter proposal vs the plain search (GPU encoder)
+# ---------------------------------------------------------------------------
+def run_learned(args, dev):
+    """Trains the proposal network on one synthetic column (2^24 values) and
+    encodes a second one of 2^26 values (the learned-proposal benchmark
+    shape: per vector d in {0..6} decimals, scale 10^k, k in 0..8, Gaussian or
+    uniform magnitude, 10% full-mantissa noise vectors) with the plain
+    per-vector search and with the network's proposals."""
+    import torch
+    import colgen
+    import flsgpu_b200 as F
+    stream = torch.cuda.current_stream()
+    n_eval = int(2 ** 26 * args.scale) // 1024 * 1024
+    train = torch.from_numpy(colgen.learned_values(101, max(1024, int(2 ** 24 * args.scale) // 1024))).to(dev)
+    evals = torch.from_numpy(colgen.learned_values(202, n_eval // 1024)).to(dev)
+    enc = F.AlpEncoder(seed=7)
+    t0 = time.perf_counter()
+    l0, l1 = enc.train(train, epochs=args.epochs, batch=1024, lr=3e-3)
+    train_s = time.perf_counter() - t0
+
+    def ev_time(fn, reps=3):
+        fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    res = {}
+    ms_plain = ev_time(lambda: res.__setitem__("plain", enc.encode(evals, 0)))
+    plain = res["plain"]
+    plain_bytes = plain.compressed_bytes
+    ms_learned = ev_time(lambda: res.__setitem__("learned", enc.encode(evals, 1)))
+    learned = res["learned"]
+    col = F.encoded_column(learned, evals.numel(), enc)
+    dec = F.decompress(col)
+    exact = bool(torch.equal(dec.view(torch.int64), evals.view(torch.int64)))
+    ms_search = ev_time(lambda: F.plain_labels(evals))
+    ms_propose = ev_time(lambda: enc.propose(evals, 3))
+    in_bytes = evals.numel() * 8
+    # the reference's CPU encoder on a bounded sample (rowgroup sampling
+    # search, one state per rowgroup of 100 vectors as upstream ALP)
+    from oracle import binding as B
+    sample = colgen.learned_values(202, 512)
+    t = time.perf_counter()
+    ref_col = B.alp_encode(sample, rowgroup_vecs=100)
+    ref_s = time.perf_counter() - t
+    return dict(ms_plain=ms_plain, ms_learned=ms_learned, ms_search=ms_search,
+                ms_propose=ms_propose, in_bytes=in_bytes, plain_bytes=plain_bytes,
+                learned_bytes=learned.compressed_bytes, fallback=int(learned.n_fallback),
+                n_rd=int(learned.n_rd), n_vecs=evals.numel() // 1024, exact=exact,
+                loss=(l0, l1), train_s=train_s,
+                ref_gbs=sample.nbytes / ref_s / 1e9 if ref_col is not None else None,
+                ref_ratio=sample.nbytes / ref_col["compressed_bytes"] if ref_col is not None else None)
+
+
+# ---------------------------------------------------------------------------
 # end-to-end through the C ABI with host buffers (bounded sample)
 # ---------------------------------------------------------------------------
 def run_e2e(args, dev):
@@ -378,7 +568,9 @@ def main():
     ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--workload", choices=["ffor", "ffor-sum"], default="ffor")
+    ap.add_argument("--workload", choices=["ffor", "ffor-sum", "batch", "learned"], default="ffor")
+    ap.add_argument("--epochs", type=int, default=12, help="learned workload: training epochs")
+    ap.add_argument("--columns", type=int, default=2000, help="batch workload: column count")
     ap.add_argument("--scale", type=float, default=1.0,
                     help="fraction of the benchmark column sizes (1.0 = full)")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
@@ -414,6 +606,73 @@ def main():
     import torch
     rank, world, local = dist_init()
     dev = torch.device("cuda", torch.cuda.current_device())
+    if args.workload == "learned":
+        r = run_learned(args, dev)
+        gbs_l = r["in_bytes"] / (r["ms_learned"] / 1e3) / 1e9
+        gbs_p = r["in_bytes"] / (r["ms_plain"] / 1e3) / 1e9
+        if rank == 0:
+            print(json.dumps({
+                "metric": "ALP encode GB/s (input bytes / end-to-end GPU encode), learned vs plain",
+                "value": round(gbs_l, 1), "unit": "GB/s", "n_gpus": world, "steps": 3,
+                "warmup": 1, "ms_per_step": round(r["ms_learned"], 3), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": "learned ALP parameter proposal: f64 column of "
+                                       f"{r['n_vecs'] * 1024} values (d in 0..6, scale 10^0..8, "
+                                       "Gaussian/uniform, 10% noise vectors); network trained "
+                                       "on a separate 2^24-value column"},
+                "learned": {"encode_gbs": round(gbs_l, 1), "ms": round(r["ms_learned"], 3),
+                            "ratio": round(r["in_bytes"] / r["learned_bytes"], 4),
+                            "fallback_vectors": r["fallback"], "rd_vectors": r["n_rd"],
+                            "proposal_ms": round(r["ms_propose"], 3),
+                            "decode_bit_exact": r["exact"]},
+                "plain": {"encode_gbs": round(gbs_p, 1), "ms": round(r["ms_plain"], 3),
+                          "ratio": round(r["in_bytes"] / r["plain_bytes"], 4),
+                          "search_ms": round(r["ms_search"], 3)},
+                "speedup_encode_vs_plain": round(r["ms_plain"] / r["ms_learned"], 2),
+                "speedup_selection_vs_plain_search": round(r["ms_search"] / r["ms_propose"], 2),
+                "ratio_loss_vs_plain": round(1 - r["plain_bytes"] / r["learned_bytes"], 4),
+                "training": {"epochs": args.epochs, "seconds": round(r["train_s"], 2),
+                             "loss_first_epoch": round(r["loss"][0], 4),
+                             "loss_last_epoch": round(r["loss"][1], 4)},
+                "cpu_baseline": {"value": round(r["ref_gbs"], 3) if r["ref_gbs"] else None,
+                                 "unit": "GB/s", "cores": 1, "kind": "port",
+                                 "ratio": round(r["ref_ratio"], 4) if r["ref_ratio"] else None,
+                                 "sample": "512 vectors, oracle restatement of alp::encode with "
+                                           "rowgroup sampling (100 vectors per state)"}}))
+        return
+    if args.workload == "batch":
+        r = run_batch(args, dev)
+        pk, pk_kind = peaks()
+        hbm = float(pk["hbm_gbs"])
+        gbs = (r["read"] + r["write"]) / (r["ms"] / 1e3) / 1e9
+        if rank == 0:
+            print(json.dumps({
+                "metric": "batched uneven decode GB/s (compressed read + decoded write), 1 B200",
+                "value": round(gbs, 1), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": round(r["ms"], 3), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "u32/f32/f64", "data": "synthetic",
+                "config": {"workload": f"batched uneven decode: {args.columns} columns, lengths "
+                                       "log-uniform 2^10..2^24 (x1024), types f64 ALP / u32 FFOR / "
+                                       "f32 ALP, one persistent launch replayed from a CUDA graph",
+                           "values": r["n_values"], "compressed_bytes": r["read"],
+                           "decoded_bytes": r["write"],
+                           "l2": "total decoded bytes exceed L2; no flush"},
+                "hbm_fraction": {"of_measured": round(gbs / hbm, 4), "of_spec_8tbs": round(gbs / 8000, 4)},
+                "per_column_launches_ms": round(r["ms_each"], 3),
+                "per_column_launches_sync_ms": round(r["ms_each_sync"], 3),
+                "eager_single_launch_ms": round(r["ms_launch"], 3),
+                "speedup_vs_per_column": round(r["ms_each"] / r["ms"], 2),
+                "speedup_vs_per_column_sync": round(r["ms_each_sync"] / r["ms"], 2),
+                "pair_query": {"pairs": r["n_pairs"], "ms": round(r["ms_query"], 3),
+                               "compressed_gbs": round(r["q_read"] / (r["ms_query"] / 1e3) / 1e9, 1),
+                               "what": "sum(A where B < median(B)) per (f64 ALP, u32 FFOR) pair, "
+                                       "4 radix passes over packed B + 1 fused decode/sum pass"},
+                "roofline": {"bound": "hbm", "achieved": round(gbs, 1), "peak": hbm, "unit": "GB/s",
+                             "frac": round(gbs / hbm, 4), "peak_kind": pk_kind,
+                             "kernel": "k_batch (flsgpu_batch_replay)", "traffic": None},
+                "gpu_launches": r["launches"], "clocks": r["clocks"],
+                "generation_s": round(r["gen_s"], 1)}))
+        return
     res = run_ffor(args, rank, world, dev)
     e2e = None if args.no_e2e else run_e2e(args, dev)
     pk, pk_kind = peaks()

@@ -1,0 +1,140 @@
+/*
+ * flsgpu_b200_ext.h -- C ABI of the parts of libflsgpu_b200.so that have no
+ * counterpart in the reference: batched persistent decode of many columns,
+ * the fused pair query over compressed columns, and the GPU ALP encoder
+ * with its learned (exponent, factor) proposal network.
+ * Conventions as in flsgpu_b200.h.
+ */
+#ifndef FLSGPU_B200_EXT_H
+#define FLSGPU_B200_EXT_H
+
+#include "flsgpu_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- batched persistent decode (no reference counterpart; replaces one
+ *      launch + cudaDeviceSynchronize per column, src/engine/kernels.cuh:
+ *      94-112) -------------------------------------------------------------
+ * Columns are grouped by value type; within a group all vectors of all
+ * columns form one index space that a persistent grid takes in chunks from
+ * an atomic counter, so a batch of columns of uneven length, type and bit
+ * width decodes in one launch per value type present (at most four).  The
+ * decode per vector is the single-column kernels' (same per-width autotuned
+ * unpackers). */
+typedef enum flsgpu_type {
+  FLSGPU_TYPE_U32 = 0, FLSGPU_TYPE_U64 = 1, FLSGPU_TYPE_F32 = 2, FLSGPU_TYPE_F64 = 3
+} flsgpu_type;
+typedef enum flsgpu_encoding {
+  FLSGPU_ENCODING_BP = 0, FLSGPU_ENCODING_FFOR = 1, FLSGPU_ENCODING_ALP = 2,
+  FLSGPU_ENCODING_ALP_EXTENDED = 3
+} flsgpu_encoding;
+typedef struct flsgpu_batch_column {
+  uint32_t type;       /* flsgpu_type */
+  uint32_t encoding;   /* flsgpu_encoding; floats need ALP, integers BP/FFOR */
+  const void *column;  /* host pointer to the matching flsgpu_*_column */
+  void *d_out;         /* device output, column n_values elements */
+} flsgpu_batch_column;
+typedef struct flsgpu_batch flsgpu_batch;
+
+/* Copies the descriptors into a device table (allocates ~200 B per column).
+ * The descriptors' device arrays must outlive the batch. */
+flsgpu_status flsgpu_batch_create(const flsgpu_batch_column *columns, size_t n_columns,
+                                  const flsgpu_decode_opts *opts, flsgpu_batch **out);
+/* One persistent launch per value type (plus counter resets). */
+flsgpu_status flsgpu_batch_decompress(flsgpu_batch *batch, flsgpu_stream stream);
+/* Captures flsgpu_batch_decompress into a CUDA graph held by the batch
+ * (NULL stream: a private stream is used); flsgpu_batch_replay launches it. */
+flsgpu_status flsgpu_batch_capture_graph(flsgpu_batch *batch, flsgpu_stream stream);
+flsgpu_status flsgpu_batch_replay(flsgpu_batch *batch, flsgpu_stream stream);
+/* The comparison path: one flsgpu_decompress_* launch per column; with
+ * sync_each the stream is synchronised after every launch, as the
+ * reference's host launchers do (src/engine/kernels.cuh:106). */
+flsgpu_status flsgpu_batch_decompress_each(flsgpu_batch *batch, int sync_each,
+                                           flsgpu_stream stream);
+size_t flsgpu_batch_total_vectors(const flsgpu_batch *batch);
+void flsgpu_batch_destroy(flsgpu_batch *batch);
+
+/* ---- fused pair query over compressed columns (no reference counterpart)
+ * For each pair i: d_results[i] = sum of A_i[k] over positions k with
+ * B_i[k] < median(B_i), where A_i is an f64 ALP column, B_i a u32 FFOR
+ * column of the same n_values, and median(B_i) the element of rank
+ * floor((n-1)/2) of B_i's values (radix select, four 8-bit passes over the
+ * packed B).  The sum follows the fixed reduction tree of flsgpu_sum_alp_f64
+ * restricted to the selected positions, so results are reproducible bit
+ * for bit.  d_medians (optional) receives each median.  At most 2^21
+ * vectors per pair. */
+typedef struct flsgpu_pair_query flsgpu_pair_query;
+flsgpu_status flsgpu_pair_query_create(const flsgpu_alp_column *a, const flsgpu_ffor_column *b,
+                                       size_t n_pairs, double *d_results, uint32_t *d_medians,
+                                       uint32_t *d_status, flsgpu_pair_query **out);
+flsgpu_status flsgpu_pair_query_run(flsgpu_pair_query *q, flsgpu_stream stream);
+flsgpu_status flsgpu_pair_query_capture_graph(flsgpu_pair_query *q, flsgpu_stream stream);
+flsgpu_status flsgpu_pair_query_replay(flsgpu_pair_query *q, flsgpu_stream stream);
+void flsgpu_pair_query_destroy(flsgpu_pair_query *q);
+
+/* ---- GPU ALP encoder (f64) with the learned parameter proposal ---------
+ * Replaces the reference's CPU alp::encode (src/alp/alp-bindings.cu:84-206)
+ * for f64 columns.  Parameters are chosen per vector: mode 0 runs the plain
+ * sampling search (all 190 (exponent, factor) pairs on the vector's 32
+ * samples, estimate and tie rules of encoder.hpp:134-230); mode 1 asks the
+ * network for its three best pairs, chooses among them with the reference's
+ * second-level rule (encoder.hpp:237-300) and falls back to the plain search
+ * when the choice leaves more than 30 exceptions (3%) in the vector or the
+ * network proposes ALP-RD.  Exceptions store the original values, so the
+ * column decodes exactly either way.  The network: 64 features of the 32
+ * samples -> 128 -> 128 -> 192 logits (190 pairs, ALP-RD, padding), BF16
+ * weights, FP32 accumulation on the tensor cores (tcgen05), trained on the
+ * GPU with Adam on the plain search's labels. */
+typedef struct flsgpu_alp_encoder flsgpu_alp_encoder;
+typedef struct flsgpu_alp_encode_result {
+  flsgpu_alp_column column;  /* device arrays in the encoder's workspace */
+  size_t n_packed_words;
+  size_t n_exceptions;
+  size_t compressed_bytes;   /* reference accounting, alp-bindings.cu:19-43 */
+  size_t n_fallback;         /* vectors that fell back to the plain search */
+  size_t n_rd;               /* vectors whose search estimate calls for ALP-RD */
+  double mean_bit_width;
+} flsgpu_alp_encode_result;
+
+flsgpu_status flsgpu_alp_encoder_create(uint32_t seed, flsgpu_alp_encoder **out);
+void flsgpu_alp_encoder_destroy(flsgpu_alp_encoder *encoder);
+/* Trains on the plain search's labels of d_values (n_values % 1024 == 0):
+ * `epochs` passes of Adam over shuffled minibatches of `batch` rows
+ * (batch % 128 == 0).  Synchronises; reports the first and last epoch's mean
+ * cross entropy. */
+flsgpu_status flsgpu_alp_encoder_train(flsgpu_alp_encoder *encoder, const double *d_values,
+                                       size_t n_values, uint32_t epochs, uint32_t batch, float lr,
+                                       float *h_loss_first, float *h_loss_last,
+                                       flsgpu_stream stream);
+flsgpu_status flsgpu_alp_encode_f64(flsgpu_alp_encoder *encoder, const double *d_values,
+                                    size_t n_values, uint32_t mode,
+                                    flsgpu_alp_encode_result *out, flsgpu_stream stream);
+/* pieces exposed for tests and tools */
+flsgpu_status flsgpu_alp_encoder_propose(flsgpu_alp_encoder *encoder, const double *d_values,
+                                         size_t n_values, uint32_t k, int16_t *d_cand,
+                                         flsgpu_stream stream);
+flsgpu_status flsgpu_alp_plain_labels(const double *d_values, size_t n_values, int16_t *d_labels,
+                                      int32_t *d_estimates, flsgpu_stream stream);
+flsgpu_status flsgpu_alp_features(const double *d_values, size_t n_values, void *d_features_bf16,
+                                  flsgpu_stream stream);
+size_t flsgpu_alp_encoder_param_count(void);
+flsgpu_status flsgpu_alp_encoder_get_params(const flsgpu_alp_encoder *encoder, float *h_params);
+flsgpu_status flsgpu_alp_encoder_set_params(flsgpu_alp_encoder *encoder, const float *h_params);
+flsgpu_status flsgpu_alp_encoder_gradients(flsgpu_alp_encoder *encoder, const void *d_features_bf16,
+                                           const int16_t *d_labels, uint32_t rows, float *d_grads,
+                                           float *h_loss, flsgpu_stream stream);
+flsgpu_status flsgpu_alp_encoder_save(const flsgpu_alp_encoder *encoder, const char *path);
+flsgpu_status flsgpu_alp_encoder_load(flsgpu_alp_encoder *encoder, const char *path);
+/* C (fp32 / bf16, M x N, row stride ldc) = A (bf16 M x K) . B (bf16 N x K)^T
+ * [+ bias][relu] on the tensor cores (tcgen05, accumulator in TMEM);
+ * N <= 256, K % 16 == 0, operands 16-byte aligned. */
+flsgpu_status flsgpu_gemm_bf16_tn(const void *A, int lda, const void *B, int ldb, int M, int N,
+                                  int K, float *Cf, void *Cb, int ldc, const float *bias, int relu,
+                                  uint32_t *d_status, flsgpu_stream stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FLSGPU_B200_EXT_H */

@@ -9,6 +9,7 @@ from __future__ import annotations
 
 import argparse
 import os
+import re
 import subprocess
 import sys
 from concurrent.futures import ThreadPoolExecutor
@@ -24,13 +25,24 @@ FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxe
          "-Xptxas", "-warn-spills", "-diag-suppress", "177,550"]
 
 
-def _headers() -> list[Path]:
-    return list(CSRC.glob("*.cuh")) + list((PKG.parent / "include").glob("*.h"))
+_INCLUDE = re.compile(r'^\s*#\s*include\s+"([^"]+)"', re.M)
+
+
+def _deps(path: Path, seen: set[Path] | None = None) -> set[Path]:
+    """The file and every local header it includes, recursively."""
+    seen = seen if seen is not None else set()
+    path = path.resolve()
+    if path in seen or not path.exists():
+        return seen
+    seen.add(path)
+    for inc in _INCLUDE.findall(path.read_text()):
+        _deps(path.parent / inc, seen)
+    return seen
 
 
 def compile_one(src: Path, force: bool, extra: list[str]) -> Path:
     obj = BUILD / (src.stem + ".o")
-    newest = max([src.stat().st_mtime] + [h.stat().st_mtime for h in _headers()])
+    newest = max(p.stat().st_mtime for p in _deps(src))
     if force or not obj.exists() or obj.stat().st_mtime < newest:
         cmd = [NVCC, *ARCH, *FLAGS, *extra, "-c", str(src), "-o", str(obj)]
         r = subprocess.run(cmd, capture_output=True, text=True)

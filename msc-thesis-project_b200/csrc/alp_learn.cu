@@ -1,0 +1,772 @@
+// alp_learn.cu -- the learned (exponent, factor) proposal for the GPU ALP
+// encoder: per-vector features, a 64 -> 128 -> 128 -> 192 MLP with BF16
+// weights and FP32 accumulation on the tensor cores (mlp.cu), trained on the
+// GPU with these kernels on labels from the plain sampling search
+// (alp_encode.cu), and the encoder API that uses it.  No counterpart in the
+// reference; it replaces encoder::init / find_top_k_combinations
+// (src/alp/encoder.hpp:134-230, :400-406) as the source of candidate pairs,
+// keeps the reference's second-level choice among candidates
+// (encoder.hpp:237-300) and falls back to the plain search whenever the
+// chosen pair leaves more than 3% exceptions, so decoding stays exact.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <random>
+#include <vector>
+
+#include "alp_learn.cuh"
+
+namespace flsb200 {
+
+static __constant__ double c_pow10_feat[17] = {1.0,  1e1,  1e2,  1e3,  1e4,  1e5,  1e6,  1e7, 1e8,
+                                               1e9,  1e10, 1e11, 1e12, 1e13, 1e14, 1e15, 1e16};
+
+__device__ __forceinline__ float warp_sum_f(float x) {
+#pragma unroll
+  for (int s = 16; s >= 1; s >>= 1) x += __shfl_xor_sync(0xffffffffu, x, s);
+  return x;
+}
+__device__ __forceinline__ float warp_min_f(float x) {
+#pragma unroll
+  for (int s = 16; s >= 1; s >>= 1) x = fminf(x, __shfl_xor_sync(0xffffffffu, x, s));
+  return x;
+}
+__device__ __forceinline__ float warp_max_f(float x) {
+#pragma unroll
+  for (int s = 16; s >= 1; s >>= 1) x = fmaxf(x, __shfl_xor_sync(0xffffffffu, x, s));
+  return x;
+}
+
+// 64 features of a vector from its 32 samples (lane i holds value 32 i, the
+// samples the search uses): magnitude moments, sign / zero / non-finite
+// fractions, histograms of the decimal digits after the point (smallest d
+// with x * 10^d integral), of trailing zero bits of the mantissa, of
+// log10|x|, and of the binary exponent.
+__global__ void __launch_bounds__(256) k_features(const double *__restrict__ vals, size_t n_vecs,
+                                                  __nv_bfloat16 *feat) {
+  const int t = threadIdx.x & 31;
+  const size_t nw = ((size_t)gridDim.x * blockDim.x) >> 5;
+  for (size_t v = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n_vecs; v += nw) {
+    const double x = vals[v * VEC + 32 * t];
+    const uint64_t bits = (uint64_t)__double_as_longlong(x);
+    const bool fin = isfinite(x);
+    const double a = fabs(x);
+    const bool nz = fin && a > 0.0;
+    const float l = nz ? (float)log10(a) : 0.0f;
+    int d = 17;
+    if (fin) {
+      for (int dd = 0; dd < 17; ++dd) {
+        const double y = __dmul_rn(x, c_pow10_feat[dd]);
+        if (fabs(y) < 9007199254740992.0 && y == rint(y)) {
+          d = dd;
+          break;
+        }
+      }
+    }
+    int tz = 53;
+    if (nz) {
+      uint64_t mant = bits & 0xFFFFFFFFFFFFFull;
+      if ((bits >> 52) & 0x7FF) mant |= 1ull << 52;
+      tz = __ffsll((long long)mant) - 1;
+    }
+    const int e2 = (int)((bits >> 52) & 0x7FF) - 1023;
+    float f[64];
+    const float nnz = (float)__popc(__ballot_sync(0xffffffffu, nz));
+    const float inv = nnz > 0 ? 1.0f / nnz : 0.0f;
+    const float mean_l = warp_sum_f(nz ? l : 0.0f) * inv;
+    const float var_l = warp_sum_f(nz ? (l - mean_l) * (l - mean_l) : 0.0f) * inv;
+    f[0] = mean_l / 10.0f;
+    f[1] = sqrtf(var_l) / 10.0f;
+    f[2] = nnz > 0 ? warp_min_f(nz ? l : 1e30f) / 10.0f : 0.0f;
+    f[3] = nnz > 0 ? warp_max_f(nz ? l : -1e30f) / 10.0f : 0.0f;
+    f[4] = __popc(__ballot_sync(0xffffffffu, fin && a == 0.0)) / 32.0f;
+    f[5] = __popc(__ballot_sync(0xffffffffu, fin && x < 0.0)) / 32.0f;
+    f[6] = __popc(__ballot_sync(0xffffffffu, !fin)) / 32.0f;
+#pragma unroll
+    for (int b = 0; b < 18; ++b) f[7 + b] = __popc(__ballot_sync(0xffffffffu, d == b)) / 32.0f;
+    const int tzb = tz >= 53 ? 16 : min(15, tz / 4);
+#pragma unroll
+    for (int b = 0; b < 17; ++b) f[25 + b] = __popc(__ballot_sync(0xffffffffu, tzb == b)) / 32.0f;
+    const int lb = nz ? max(0, min(7, (int)floorf((l + 12.0f) / 4.0f))) : -1;
+#pragma unroll
+    for (int b = 0; b < 8; ++b) f[42 + b] = __popc(__ballot_sync(0xffffffffu, lb == b)) / 32.0f;
+    f[50] = warp_sum_f((float)d) / (32.0f * 17.0f);
+    f[51] = warp_max_f((float)d) / 17.0f;
+    f[52] = warp_min_f((float)d) / 17.0f;
+    f[53] = f[7];
+    const float me = warp_sum_f((float)e2) / 32.0f;
+    f[54] = me / 64.0f;
+    f[55] = sqrtf(warp_sum_f(((float)e2 - me) * ((float)e2 - me)) / 32.0f) / 64.0f;
+    f[56] = warp_min_f((float)e2) / 1024.0f;
+    f[57] = warp_max_f((float)e2) / 1024.0f;
+#pragma unroll
+    for (int j = 0; j < 6; ++j)
+      f[58 + j] = __popc(__ballot_sync(0xffffffffu, d <= 2 + 2 * j)) / 32.0f;
+    float lo = 0.0f, hi = 0.0f;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      if (t == j) {
+        lo = f[j];
+        hi = f[j + 32];
+      }
+    }
+    feat[v * kFeatures + t] = __float2bfloat16_rn(lo);
+    feat[v * kFeatures + 32 + t] = __float2bfloat16_rn(hi);
+  }
+}
+
+// Softmax cross entropy over the 191 real classes of each row (class 191
+// is padding): loss[row] and dZ = (softmax - onehot) / rows (bf16).
+__global__ void k_softmax_ce(const float *__restrict__ z, const int16_t *__restrict__ labels,
+                             int rows, float *loss, __nv_bfloat16 *dz) {
+  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int t = threadIdx.x & 31;
+  if (row >= rows) return;
+  const float *zr = z + (size_t)row * kOut;
+  float m = -1e30f;
+  for (int c = t; c < kClasses; c += 32) m = fmaxf(m, zr[c]);
+  m = warp_max_f(m);
+  float s = 0.0f;
+  for (int c = t; c < kClasses; c += 32) s += __expf(zr[c] - m);
+  s = warp_sum_f(s);
+  const int y = labels[row];
+  const float inv_rows = 1.0f / (float)rows;
+  for (int c = t; c < kOut; c += 32) {
+    float g = 0.0f;
+    if (c < kClasses) g = (__expf(zr[c] - m) / s - (c == y ? 1.0f : 0.0f)) * inv_rows;
+    dz[(size_t)row * kOut + c] = __float2bfloat16_rn(g);
+  }
+  if (t == 0) loss[row] = -(zr[y] - m - __logf(s));
+}
+
+// out[c][r] = in[r][c] (bf16), rows x cols -> cols x ld_out
+__global__ void k_transpose_bf16(const __nv_bfloat16 *__restrict__ in, int rows, int cols,
+                                 int ld_in, __nv_bfloat16 *out, int ld_out) {
+  __shared__ __nv_bfloat16 tile[32][33];
+  const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+  for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+    const int r = r0 + i, c = c0 + threadIdx.x;
+    tile[i][threadIdx.x] = (r < rows && c < cols) ? in[(size_t)r * ld_in + c] : __float2bfloat16_rn(0.f);
+  }
+  __syncthreads();
+  for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+    const int c = c0 + i, r = r0 + threadIdx.x;
+    if (c < cols && r < rows) out[(size_t)c * ld_out + r] = tile[threadIdx.x][i];
+  }
+}
+
+// dX (bf16) = dXf * (H > 0): the ReLU derivative applied to an fp32 gradient
+__global__ void k_relu_back(const float *__restrict__ dxf, const __nv_bfloat16 *__restrict__ h,
+                            int rows, int cols, __nv_bfloat16 *dx) {
+  const size_t n = (size_t)rows * cols;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const float g = __bfloat162float(h[i]) > 0.0f ? dxf[i] : 0.0f;
+    dx[i] = __float2bfloat16_rn(g);
+  }
+}
+
+// db[c] = sum over rows of g[r][c] (g bf16), one thread per column
+__global__ void k_colsum_bf16(const __nv_bfloat16 *__restrict__ g, int rows, int cols, float *db) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= cols) return;
+  float s = 0.0f;
+  for (int r = 0; r < rows; ++r) s += __bfloat162float(g[(size_t)r * cols + c]);
+  db[c] = s;
+}
+
+// Adam on fp32 master parameters; refreshes the bf16 copy (and its
+// transpose when wt != nullptr; rows x cols row-major).
+__global__ void k_adam(float *w, const float *g, float *m, float *v, int n, float lr, float b1,
+                       float b2, float eps, float c1, float c2, __nv_bfloat16 *wb,
+                       __nv_bfloat16 *wt, int rows, int cols) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float gi = g[i];
+  const float mi = b1 * m[i] + (1.0f - b1) * gi;
+  const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+  m[i] = mi;
+  v[i] = vi;
+  const float wi = w[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+  w[i] = wi;
+  if (wb) wb[i] = __float2bfloat16_rn(wi);
+  if (wt) {
+    const int r = i / cols, c = i % cols;
+    wt[(size_t)c * rows + r] = __float2bfloat16_rn(wi);
+  }
+}
+
+__global__ void k_to_bf16(const float *w, int n, __nv_bfloat16 *wb, __nv_bfloat16 *wt, int rows,
+                          int cols) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  wb[i] = __float2bfloat16_rn(w[i]);
+  if (wt) {
+    const int r = i / cols, c = i % cols;
+    wt[(size_t)c * rows + r] = __float2bfloat16_rn(w[i]);
+  }
+}
+
+// Top-k (k <= 4) classes of each row of the logits, best first; ties keep
+// the smaller class.  One warp per row.
+__global__ void k_topk(const float *__restrict__ z, int rows, int k, int16_t *cand) {
+  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int t = threadIdx.x & 31;
+  if (row >= rows) return;
+  const float *zr = z + (size_t)row * kOut;
+  unsigned long long taken = 0ull, taken2 = 0ull, taken3 = 0ull, taken4 = 0ull;
+  for (int j = 0; j < k; ++j) {
+    float bv = -1e30f;
+    int bc = 1 << 20;
+    for (int c = t; c < kClasses; c += 32) {
+      const int word = c >> 6, bit = c & 63;
+      const unsigned long long tk = word == 0 ? taken : word == 1 ? taken2 : word == 2 ? taken3 : taken4;
+      if ((tk >> bit) & 1ull) continue;
+      const float val = zr[c];
+      if (val > bv || (val == bv && c < bc)) {
+        bv = val;
+        bc = c;
+      }
+    }
+#pragma unroll
+    for (int s = 16; s >= 1; s >>= 1) {
+      const float ov = __shfl_xor_sync(0xffffffffu, bv, s);
+      const int oc = __shfl_xor_sync(0xffffffffu, bc, s);
+      if (ov > bv || (ov == bv && oc < bc)) {
+        bv = ov;
+        bc = oc;
+      }
+    }
+    if (t == 0) cand[(size_t)row * k + j] = (int16_t)bc;
+    const int word = bc >> 6, bit = bc & 63;
+    if (word == 0) taken |= 1ull << bit;
+    else if (word == 1) taken2 |= 1ull << bit;
+    else if (word == 2) taken3 |= 1ull << bit;
+    else taken4 |= 1ull << bit;
+  }
+}
+
+}  // namespace flsb200
+
+// ---------------------------------------------------------------------------
+// host side: the encoder object
+// ---------------------------------------------------------------------------
+namespace {
+
+using namespace flsb200;
+using bf16 = __nv_bfloat16;
+
+// parameter layout in one fp32 array (also the save-file payload)
+constexpr int kW1 = kHidden * kFeatures, kB1 = kHidden;
+constexpr int kW2 = kHidden * kHidden, kB2 = kHidden;
+constexpr int kW3 = kOut * kHidden, kB3 = kOut;
+constexpr int kOffW1 = 0, kOffB1 = kOffW1 + kW1, kOffW2 = kOffB1 + kB1, kOffB2 = kOffW2 + kW2,
+              kOffB2End = kOffB2 + kB2, kOffW3 = kOffB2End, kOffB3 = kOffW3 + kW3,
+              kParams = kOffB3 + kB3;
+
+template <typename T> T *dalloc(size_t n, flsgpu_status &st) {
+  void *p = nullptr;
+  if (st == FLSGPU_OK) st = check_cuda(cudaMalloc(&p, (n ? n : 1) * sizeof(T) + 16), "cudaMalloc");
+  return static_cast<T *>(p);
+}
+
+}  // namespace
+
+struct flsgpu_alp_encoder {
+  // parameters (fp32 master), Adam moments, gradients
+  float *w = nullptr, *m = nullptr, *v = nullptr, *g = nullptr;
+  bf16 *w1b = nullptr, *w2b = nullptr, *w3b = nullptr;  // bf16 copies
+  bf16 *w2t = nullptr, *w3t = nullptr;                  // bf16 transposes
+  // activations of one batch
+  int cap_rows = 0;
+  bf16 *x = nullptr, *h1 = nullptr, *h2 = nullptr, *dz = nullptr;
+  float *z = nullptr, *tmpf = nullptr, *loss = nullptr;
+  bf16 *dh = nullptr, *t_a = nullptr, *t_b = nullptr;
+  uint32_t *status = nullptr;
+  int adam_t = 0;
+  // encode workspaces (sized for cap_vecs vectors)
+  size_t cap_vecs = 0;
+  bf16 *feat = nullptr;
+  int16_t *labels = nullptr, *cand = nullptr;
+  EncodeSlots sl{};
+  size_t *off_words = nullptr, *off_exc = nullptr, *totals = nullptr;
+  uint64_t *packed = nullptr;
+  double *exc = nullptr;
+  uint16_t *pos = nullptr;
+  size_t *exc_offs = nullptr, *vec_offs = nullptr;
+};
+
+namespace {
+
+void free_acts(flsgpu_alp_encoder *e) {
+  for (void *p : {(void *)e->x, (void *)e->h1, (void *)e->h2, (void *)e->dz, (void *)e->z,
+                  (void *)e->tmpf, (void *)e->loss, (void *)e->dh, (void *)e->t_a, (void *)e->t_b})
+    if (p) cudaFree(p);
+  e->x = e->h1 = e->h2 = e->dz = e->dh = e->t_a = e->t_b = nullptr;
+  e->z = e->tmpf = e->loss = nullptr;
+  e->cap_rows = 0;
+}
+
+flsgpu_status ensure_rows(flsgpu_alp_encoder *e, int rows) {
+  if (rows <= e->cap_rows) return FLSGPU_OK;
+  free_acts(e);
+  flsgpu_status st = FLSGPU_OK;
+  const size_t r = (size_t)((rows + 127) / 128 * 128);
+  e->x = dalloc<bf16>(r * kFeatures, st);
+  e->h1 = dalloc<bf16>(r * kHidden, st);
+  e->h2 = dalloc<bf16>(r * kHidden, st);
+  e->dz = dalloc<bf16>(r * kOut, st);
+  e->z = dalloc<float>(r * kOut, st);
+  e->tmpf = dalloc<float>(r * kOut, st);
+  e->loss = dalloc<float>(r, st);
+  e->dh = dalloc<bf16>(r * kOut, st);
+  e->t_a = dalloc<bf16>(r * kOut, st);
+  e->t_b = dalloc<bf16>(r * kOut, st);
+  if (st == FLSGPU_OK) e->cap_rows = (int)r;
+  return st;
+}
+
+void free_enc(flsgpu_alp_encoder *e) {
+  for (void *p : {(void *)e->feat, (void *)e->labels, (void *)e->cand, (void *)e->sl.packed,
+                  (void *)e->sl.exc, (void *)e->sl.pos, (void *)e->sl.bw, (void *)e->sl.base,
+                  (void *)e->sl.fac, (void *)e->sl.exp, (void *)e->sl.count, (void *)e->sl.flags,
+                  (void *)e->off_words, (void *)e->off_exc, (void *)e->totals, (void *)e->packed,
+                  (void *)e->exc, (void *)e->pos})
+    if (p) cudaFree(p);
+  e->feat = nullptr;
+  e->labels = e->cand = nullptr;
+  e->sl = EncodeSlots{};
+  e->off_words = e->off_exc = e->totals = nullptr;
+  e->packed = nullptr;
+  e->exc = nullptr;
+  e->pos = nullptr;
+  e->cap_vecs = 0;
+}
+
+flsgpu_status ensure_vecs(flsgpu_alp_encoder *e, size_t n_vecs) {
+  if (n_vecs <= e->cap_vecs) return FLSGPU_OK;
+  free_enc(e);
+  flsgpu_status st = FLSGPU_OK;
+  const size_t n = n_vecs;
+  e->feat = dalloc<bf16>(n * kFeatures, st);
+  e->labels = dalloc<int16_t>(n, st);
+  e->cand = dalloc<int16_t>(n * 4, st);
+  e->sl.packed = dalloc<uint64_t>(n * VEC, st);
+  e->sl.exc = dalloc<double>(n * VEC, st);
+  e->sl.pos = dalloc<uint16_t>(n * VEC, st);
+  e->sl.bw = dalloc<uint8_t>(n, st);
+  e->sl.base = dalloc<uint64_t>(n, st);
+  e->sl.fac = dalloc<uint8_t>(n, st);
+  e->sl.exp = dalloc<uint8_t>(n, st);
+  e->sl.count = dalloc<uint16_t>(n, st);
+  e->sl.flags = dalloc<uint8_t>(n, st);
+  e->off_words = dalloc<size_t>(n, st);
+  e->off_exc = dalloc<size_t>(n, st);
+  e->totals = dalloc<size_t>(4, st);
+  e->packed = dalloc<uint64_t>(n * VEC, st);
+  e->exc = dalloc<double>(n * VEC, st);
+  e->pos = dalloc<uint16_t>(n * VEC, st);
+  if (st == FLSGPU_OK) e->cap_vecs = n;
+  return st;
+}
+
+flsgpu_status refresh_bf16(flsgpu_alp_encoder *e, cudaStream_t s) {
+  k_to_bf16<<<(kW1 + 255) / 256, 256, 0, s>>>(e->w + kOffW1, kW1, e->w1b, nullptr, kHidden, kFeatures);
+  k_to_bf16<<<(kW2 + 255) / 256, 256, 0, s>>>(e->w + kOffW2, kW2, e->w2b, e->w2t, kHidden, kHidden);
+  k_to_bf16<<<(kW3 + 255) / 256, 256, 0, s>>>(e->w + kOffW3, kW3, e->w3b, e->w3t, kOut, kHidden);
+  note_launch(3);
+  return check_cuda(cudaGetLastError(), "refresh weights");
+}
+
+GemmArgs gemm(const bf16 *A, int lda, const bf16 *B, int ldb, int M, int N, int K, float *Cf,
+              bf16 *Cb, int ldc, const float *bias, int relu, uint32_t *status) {
+  return GemmArgs{A, B, lda, ldb, M, N, K, Cf, Cb, ldc, bias, relu, status};
+}
+
+// forward of `rows` feature rows already in e->x: h1, h2 (bf16), z (fp32)
+flsgpu_status forward(flsgpu_alp_encoder *e, const bf16 *x, int rows, cudaStream_t s) {
+  flsgpu_status st;
+  if ((st = gemm_tn(gemm(x, kFeatures, e->w1b, kFeatures, rows, kHidden, kFeatures, nullptr, e->h1,
+                         kHidden, e->w + kOffB1, 1, e->status), s)))
+    return st;
+  if ((st = gemm_tn(gemm(e->h1, kHidden, e->w2b, kHidden, rows, kHidden, kHidden, nullptr, e->h2,
+                         kHidden, e->w + kOffB2, 1, e->status), s)))
+    return st;
+  return gemm_tn(gemm(e->h2, kHidden, e->w3b, kHidden, rows, kOut, kHidden, e->z, nullptr, kOut,
+                      e->w + kOffB3, 0, e->status), s);
+}
+
+void transpose(const bf16 *in, int rows, int cols, bf16 *out, int ld_out, cudaStream_t s) {
+  dim3 grid((cols + 31) / 32, (rows + 31) / 32), block(32, 8);
+  k_transpose_bf16<<<grid, block, 0, s>>>(in, rows, cols, cols, out, ld_out);
+  note_launch();
+}
+
+// forward + backward of one batch (rows % 16 == 0): gradients into e->g,
+// per-row losses into e->loss
+flsgpu_status forward_backward(flsgpu_alp_encoder *e, const bf16 *x, const int16_t *labels,
+                               int rows, cudaStream_t s) {
+  flsgpu_status st;
+  if ((st = forward(e, x, rows, s))) return st;
+  const int wb = (rows * 32 + 255) / 256;
+  k_softmax_ce<<<wb, 256, 0, s>>>(e->z, labels, rows, e->loss, e->dz);
+  note_launch();
+  // layer 3: dW3 = dZ^T H2 ; db3 = colsum dZ ; dH2 = dZ W3
+  transpose(e->dz, rows, kOut, e->t_a, rows, s);     // dZ^T [192 x rows]
+  transpose(e->h2, rows, kHidden, e->t_b, rows, s);  // H2^T [128 x rows]
+  if ((st = gemm_tn(gemm(e->t_a, rows, e->t_b, rows, kOut, kHidden, rows, e->g + kOffW3, nullptr,
+                         kHidden, nullptr, 0, e->status), s)))
+    return st;
+  k_colsum_bf16<<<1, kOut, 0, s>>>(e->dz, rows, kOut, e->g + kOffB3);
+  if ((st = gemm_tn(gemm(e->dz, kOut, e->w3t, kOut, rows, kHidden, kOut, e->tmpf, nullptr, kHidden,
+                         nullptr, 0, e->status), s)))
+    return st;
+  k_relu_back<<<592, 256, 0, s>>>(e->tmpf, e->h2, rows, kHidden, e->dh);
+  // layer 2: dW2 = dH2^T H1 ; db2 ; dH1 = dH2 W2
+  transpose(e->dh, rows, kHidden, e->t_a, rows, s);
+  transpose(e->h1, rows, kHidden, e->t_b, rows, s);
+  if ((st = gemm_tn(gemm(e->t_a, rows, e->t_b, rows, kHidden, kHidden, rows, e->g + kOffW2, nullptr,
+                         kHidden, nullptr, 0, e->status), s)))
+    return st;
+  k_colsum_bf16<<<1, kHidden, 0, s>>>(e->dh, rows, kHidden, e->g + kOffB2);
+  if ((st = gemm_tn(gemm(e->dh, kHidden, e->w2t, kHidden, rows, kHidden, kHidden, e->tmpf, nullptr,
+                         kHidden, nullptr, 0, e->status), s)))
+    return st;
+  k_relu_back<<<592, 256, 0, s>>>(e->tmpf, e->h1, rows, kHidden, e->dh);
+  // layer 1: dW1 = dH1^T X ; db1
+  transpose(e->dh, rows, kHidden, e->t_a, rows, s);
+  transpose(x, rows, kFeatures, e->t_b, rows, s);
+  if ((st = gemm_tn(gemm(e->t_a, rows, e->t_b, rows, kHidden, kFeatures, rows, e->g + kOffW1,
+                         nullptr, kFeatures, nullptr, 0, e->status), s)))
+    return st;
+  k_colsum_bf16<<<1, kHidden, 0, s>>>(e->dh, rows, kHidden, e->g + kOffB1);
+  note_launch(5);
+  return check_cuda(cudaGetLastError(), "backward");
+}
+
+flsgpu_status adam_step(flsgpu_alp_encoder *e, float lr, cudaStream_t s) {
+  e->adam_t++;
+  const float b1 = 0.9f, b2 = 0.999f;
+  const float c1 = 1.0f - powf(b1, (float)e->adam_t), c2 = 1.0f - powf(b2, (float)e->adam_t);
+  struct P {
+    int off, n, rows, cols;
+    bf16 *wb, *wt;
+  } ps[6] = {{kOffW1, kW1, kHidden, kFeatures, e->w1b, nullptr}, {kOffB1, kB1, 1, kB1, nullptr, nullptr},
+             {kOffW2, kW2, kHidden, kHidden, e->w2b, e->w2t},     {kOffB2, kB2, 1, kB2, nullptr, nullptr},
+             {kOffW3, kW3, kOut, kHidden, e->w3b, e->w3t},        {kOffB3, kB3, 1, kB3, nullptr, nullptr}};
+  for (const P &p : ps) {
+    k_adam<<<(p.n + 255) / 256, 256, 0, s>>>(e->w + p.off, e->g + p.off, e->m + p.off, e->v + p.off,
+                                             p.n, lr, b1, b2, 1e-8f, c1, c2, p.wb, p.wt, p.rows, p.cols);
+  }
+  note_launch(6);
+  return check_cuda(cudaGetLastError(), "adam");
+}
+
+flsgpu_status features(const double *vals, size_t n_vecs, bf16 *feat, cudaStream_t s) {
+  if (!n_vecs) return FLSGPU_OK;
+  k_features<<<persistent_blocks(n_vecs, 8, 4), 256, 0, s>>>(vals, n_vecs, feat);
+  note_launch();
+  return check_cuda(cudaGetLastError(), "k_features");
+}
+
+flsgpu_status propose(flsgpu_alp_encoder *e, const double *vals, size_t n_vecs, int k,
+                      cudaStream_t s) {
+  flsgpu_status st;
+  if ((st = features(vals, n_vecs, e->feat, s))) return st;
+  const int chunk = 1 << 16;
+  if ((st = ensure_rows(e, (int)std::min<size_t>(n_vecs, chunk)))) return st;
+  for (size_t r0 = 0; r0 < n_vecs; r0 += chunk) {
+    const int rows = (int)std::min<size_t>(chunk, n_vecs - r0);
+    if ((st = forward(e, e->feat + r0 * kFeatures, rows, s))) return st;
+    k_topk<<<(rows * 32 + 255) / 256, 256, 0, s>>>(e->z, rows, k, e->cand + r0 * k);
+    note_launch();
+  }
+  return check_cuda(cudaGetLastError(), "propose");
+}
+
+}  // namespace
+
+extern "C" {
+
+flsgpu_status flsgpu_alp_encoder_create(uint32_t seed, flsgpu_alp_encoder **out) {
+  if (!out) return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "null output");
+  auto *e = new flsgpu_alp_encoder();
+  flsgpu_status st = FLSGPU_OK;
+  e->w = dalloc<float>(kParams, st);
+  e->m = dalloc<float>(kParams, st);
+  e->v = dalloc<float>(kParams, st);
+  e->g = dalloc<float>(kParams, st);
+  e->w1b = dalloc<bf16>(kW1, st);
+  e->w2b = dalloc<bf16>(kW2, st);
+  e->w3b = dalloc<bf16>(kW3, st);
+  e->w2t = dalloc<bf16>(kW2, st);
+  e->w3t = dalloc<bf16>(kW3, st);
+  e->status = dalloc<uint32_t>(1, st);
+  if (st == FLSGPU_OK) {
+    // He-uniform initialisation, zero biases; the padding class gets a
+    // large negative bias so it is never proposed
+    std::vector<float> h(kParams, 0.0f);
+    std::mt19937 rng(seed);
+    auto fill = [&](int off, int n, int fan_in) {
+      std::uniform_real_distribution<float> d(-std::sqrt(6.0f / fan_in), std::sqrt(6.0f / fan_in));
+      for (int i = 0; i < n; ++i) h[off + i] = d(rng);
+    };
+    fill(kOffW1, kW1, kFeatures);
+    fill(kOffW2, kW2, kHidden);
+    fill(kOffW3, kW3, kHidden);
+    for (int c = 0; c < kHidden; ++c) h[kOffW3 + (kOut - 1) * kHidden + c] = 0.0f;
+    h[kOffB3 + kOut - 1] = -30.0f;
+    st = check_cuda(cudaMemcpy(e->w, h.data(), sizeof(float) * kParams, cudaMemcpyHostToDevice), "copy");
+    if (!st) st = check_cuda(cudaMemset(e->m, 0, sizeof(float) * kParams), "memset");
+    if (!st) st = check_cuda(cudaMemset(e->v, 0, sizeof(float) * kParams), "memset");
+    if (!st) st = check_cuda(cudaMemset(e->status, 0, 4), "memset");
+    if (!st) st = refresh_bf16(e, nullptr);
+    if (!st) st = check_cuda(cudaDeviceSynchronize(), "sync");
+  }
+  if (st) {
+    flsgpu_alp_encoder_destroy(e);
+    return st;
+  }
+  *out = e;
+  return FLSGPU_OK;
+}
+
+void flsgpu_alp_encoder_destroy(flsgpu_alp_encoder *e) {
+  if (!e) return;
+  free_acts(e);
+  free_enc(e);
+  for (void *p : {(void *)e->w, (void *)e->m, (void *)e->v, (void *)e->g, (void *)e->w1b,
+                  (void *)e->w2b, (void *)e->w3b, (void *)e->w2t, (void *)e->w3t, (void *)e->status})
+    if (p) cudaFree(p);
+  delete e;
+}
+
+size_t flsgpu_alp_encoder_param_count(void) { return kParams; }
+
+flsgpu_status flsgpu_alp_encoder_get_params(const flsgpu_alp_encoder *e, float *h_params) {
+  if (!e || !h_params) return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "null argument");
+  return check_cuda(cudaMemcpy(h_params, e->w, sizeof(float) * kParams, cudaMemcpyDeviceToHost), "copy");
+}
+
+flsgpu_status flsgpu_alp_encoder_set_params(flsgpu_alp_encoder *e, const float *h_params) {
+  if (!e || !h_params) return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "null argument");
+  flsgpu_status st =
+      check_cuda(cudaMemcpy(e->w, h_params, sizeof(float) * kParams, cudaMemcpyHostToDevice), "copy");
+  if (!st) st = refresh_bf16(e, nullptr);
+  if (!st) st = check_cuda(cudaDeviceSynchronize(), "sync");
+  return st;
+}
+
+// Gradients of the mean cross entropy of `rows` labelled feature rows
+// (d_features: rows x 64 bf16) with respect to every parameter, written to
+// d_grads (flsgpu_alp_encoder_param_count() floats, the parameter layout);
+// *h_loss receives the mean loss.  Synchronises.
+flsgpu_status flsgpu_alp_encoder_gradients(flsgpu_alp_encoder *e, const void *d_features,
+                                           const int16_t *d_labels, uint32_t rows, float *d_grads,
+                                           float *h_loss, flsgpu_stream stream) {
+  if (!e || !d_features || !d_labels || !rows || (rows % 16))
+    return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "gradients: rows must be a positive multiple of 16");
+  cudaStream_t s = (cudaStream_t)stream;
+  flsgpu_status st = ensure_rows(e, (int)rows);
+  if (!st) st = forward_backward(e, static_cast<const bf16 *>(d_features), d_labels, (int)rows, s);
+  if (!st && d_grads)
+    st = check_cuda(cudaMemcpyAsync(d_grads, e->g, sizeof(float) * kParams, cudaMemcpyDeviceToDevice, s), "copy");
+  if (!st) st = check_cuda(cudaStreamSynchronize(s), "sync");
+  if (!st && h_loss) {
+    std::vector<float> l(rows);
+    st = check_cuda(cudaMemcpy(l.data(), e->loss, sizeof(float) * rows, cudaMemcpyDeviceToHost), "copy");
+    double acc = 0;
+    for (float x : l) acc += x;
+    *h_loss = (float)(acc / rows);
+  }
+  return st;
+}
+
+flsgpu_status flsgpu_alp_features(const double *d_values, size_t n_values, void *d_features,
+                                  flsgpu_stream stream) {
+  if (n_values % VEC) return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "n_values must be a multiple of 1024");
+  return features(d_values, n_values / VEC, static_cast<bf16 *>(d_features), (cudaStream_t)stream);
+}
+
+flsgpu_status flsgpu_alp_plain_labels(const double *d_values, size_t n_values, int16_t *d_labels,
+                                      int32_t *d_est, flsgpu_stream stream) {
+  if (n_values % VEC) return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "n_values must be a multiple of 1024");
+  return run_plain_labels(d_values, n_values / VEC, d_labels, d_est, (cudaStream_t)stream);
+}
+
+// Trains the network on the plain search's labels of `d_values` (features
+// and labels computed on the GPU), `epochs` passes of Adam over shuffled
+// minibatches of `batch` rows.  Synchronises; reports the mean loss of the
+// first and the last epoch.
+flsgpu_status flsgpu_alp_encoder_train(flsgpu_alp_encoder *e, const double *d_values,
+                                       size_t n_values, uint32_t epochs, uint32_t batch, float lr,
+                                       float *h_loss_first, float *h_loss_last,
+                                       flsgpu_stream stream) {
+  if (!e || !d_values || (n_values % VEC) || !batch || (batch % 128))
+    return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "train: n_values % 1024 and batch % 128 must be 0");
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t n_vecs = n_values / VEC;
+  flsgpu_status st = ensure_vecs(e, n_vecs);
+  if (!st) st = ensure_rows(e, (int)batch);
+  if (!st) st = features(d_values, n_vecs, e->feat, s);
+  if (!st) st = run_plain_labels(d_values, n_vecs, e->labels, nullptr, s);
+  if (st) return st;
+  // shuffled copies of the rows per epoch are gathered on the host side
+  // from a permutation applied to the (small) feature and label arrays
+  std::vector<bf16> hf(n_vecs * kFeatures);
+  std::vector<int16_t> hl(n_vecs);
+  if ((st = check_cuda(cudaMemcpyAsync(hf.data(), e->feat, sizeof(bf16) * hf.size(), cudaMemcpyDeviceToHost, s), "copy")) ||
+      (st = check_cuda(cudaMemcpyAsync(hl.data(), e->labels, sizeof(int16_t) * hl.size(), cudaMemcpyDeviceToHost, s), "copy")) ||
+      (st = check_cuda(cudaStreamSynchronize(s), "sync")))
+    return st;
+  std::mt19937 rng(1234);
+  std::vector<size_t> perm(n_vecs);
+  for (size_t i = 0; i < n_vecs; ++i) perm[i] = i;
+  const size_t nb = n_vecs / batch;
+  if (nb == 0) return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "fewer vectors than one batch");
+  std::vector<bf16> sf(nb * batch * kFeatures);
+  std::vector<int16_t> sl(nb * batch);
+  bf16 *dfeat = nullptr;
+  int16_t *dlab = nullptr;
+  st = check_cuda(cudaMalloc(&dfeat, sizeof(bf16) * sf.size()), "cudaMalloc");
+  if (!st) st = check_cuda(cudaMalloc(&dlab, sizeof(int16_t) * sl.size()), "cudaMalloc");
+  std::vector<float> lbuf(batch);
+  for (uint32_t ep = 0; ep < epochs && !st; ++ep) {
+    std::shuffle(perm.begin(), perm.end(), rng);
+    for (size_t i = 0; i < nb * batch; ++i) {
+      std::memcpy(&sf[i * kFeatures], &hf[perm[i] * kFeatures], sizeof(bf16) * kFeatures);
+      sl[i] = hl[perm[i]];
+    }
+    st = check_cuda(cudaMemcpyAsync(dfeat, sf.data(), sizeof(bf16) * sf.size(), cudaMemcpyHostToDevice, s), "copy");
+    if (!st) st = check_cuda(cudaMemcpyAsync(dlab, sl.data(), sizeof(int16_t) * sl.size(), cudaMemcpyHostToDevice, s), "copy");
+    double eloss = 0;
+    for (size_t b = 0; b < nb && !st; ++b) {
+      st = forward_backward(e, dfeat + b * batch * kFeatures, dlab + b * batch, (int)batch, s);
+      if (!st) st = adam_step(e, lr, s);
+      if (!st && (ep == 0 || ep + 1 == epochs)) {
+        st = check_cuda(cudaMemcpyAsync(lbuf.data(), e->loss, sizeof(float) * batch, cudaMemcpyDeviceToHost, s), "copy");
+        if (!st) st = check_cuda(cudaStreamSynchronize(s), "sync");
+        for (float x : lbuf) eloss += x;
+      }
+    }
+    if (!st && ep == 0 && h_loss_first) *h_loss_first = (float)(eloss / (nb * batch));
+    if (!st && ep + 1 == epochs && h_loss_last) *h_loss_last = (float)(eloss / (nb * batch));
+  }
+  if (!st) st = check_cuda(cudaStreamSynchronize(s), "sync");
+  cudaFree(dfeat);
+  cudaFree(dlab);
+  uint32_t hst = 0;
+  if (!st) cudaMemcpy(&hst, e->status, 4, cudaMemcpyDeviceToHost);
+  if (!st && hst) st = set_error(FLSGPU_ERR_TIMEOUT, "tensor-core wait gave up (status %x)", hst);
+  return st;
+}
+
+// Top-k (k <= 4) proposed classes per vector (d_cand: n_vecs x k int16).
+flsgpu_status flsgpu_alp_encoder_propose(flsgpu_alp_encoder *e, const double *d_values,
+                                         size_t n_values, uint32_t k, int16_t *d_cand,
+                                         flsgpu_stream stream) {
+  if (!e || !d_values || (n_values % VEC) || k < 1 || k > 4)
+    return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "propose: bad arguments");
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t n_vecs = n_values / VEC;
+  flsgpu_status st = ensure_vecs(e, n_vecs);
+  if (!st) st = propose(e, d_values, n_vecs, (int)k, s);
+  if (!st && d_cand)
+    st = check_cuda(cudaMemcpyAsync(d_cand, e->cand, sizeof(int16_t) * n_vecs * k, cudaMemcpyDeviceToDevice, s), "copy");
+  return st;
+}
+
+flsgpu_status flsgpu_alp_encoder_save(const flsgpu_alp_encoder *e, const char *path) {
+  if (!e || !path) return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "null argument");
+  std::vector<float> h(kParams);
+  flsgpu_status st = flsgpu_alp_encoder_get_params(e, h.data());
+  if (st) return st;
+  FILE *f = fopen(path, "wb");
+  if (!f) return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "cannot open %s", path);
+  const char magic[8] = {'F', 'L', 'S', 'A', 'L', 'P', 'N', '1'};
+  const uint32_t dims[4] = {kFeatures, kHidden, kHidden, kOut};
+  const bool ok = fwrite(magic, 1, 8, f) == 8 && fwrite(dims, 4, 4, f) == 4 &&
+                  fwrite(h.data(), sizeof(float), kParams, f) == (size_t)kParams;
+  fclose(f);
+  return ok ? FLSGPU_OK : set_error(FLSGPU_ERR_INVALID_ARGUMENT, "short write to %s", path);
+}
+
+flsgpu_status flsgpu_alp_encoder_load(flsgpu_alp_encoder *e, const char *path) {
+  if (!e || !path) return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "null argument");
+  FILE *f = fopen(path, "rb");
+  if (!f) return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "cannot open %s", path);
+  char magic[8];
+  uint32_t dims[4];
+  std::vector<float> h(kParams);
+  const bool ok = fread(magic, 1, 8, f) == 8 && std::memcmp(magic, "FLSALPN1", 8) == 0 &&
+                  fread(dims, 4, 4, f) == 4 && dims[0] == kFeatures && dims[1] == kHidden &&
+                  dims[2] == kHidden && dims[3] == kOut &&
+                  fread(h.data(), sizeof(float), kParams, f) == (size_t)kParams;
+  fclose(f);
+  if (!ok) return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "%s is not a proposal network file", path);
+  return flsgpu_alp_encoder_set_params(e, h.data());
+}
+
+// Encodes an f64 column (n_values % 1024 == 0) into the reference's
+// ALPColumn layout on the device.  mode 0: plain per-vector search;
+// mode 1: the network's top-3 pairs, verified on the vector's samples, with
+// the plain search as fallback above 3% exceptions.  The column's arrays
+// live in the encoder's workspace until its next encode.  Synchronises to
+// read the sizes.
+flsgpu_status flsgpu_alp_encode_f64(flsgpu_alp_encoder *e, const double *d_values,
+                                    size_t n_values, uint32_t mode,
+                                    flsgpu_alp_encode_result *out, flsgpu_stream stream) {
+  if (!e || !d_values || !out || (n_values % VEC) || mode > 1)
+    return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "encode: bad arguments");
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t n_vecs = n_values / VEC;
+  flsgpu_status st = ensure_vecs(e, n_vecs);
+  if (st) return st;
+  if (mode == 1 && (st = propose(e, d_values, n_vecs, 3, s))) return st;
+  if ((st = run_alp_encode(d_values, n_vecs, (int)mode, e->cand, 3, 30, e->sl, e->off_words,
+                           e->off_exc, e->totals, e->packed, e->exc, e->pos, s)))
+    return st;
+  size_t tot[2] = {0, 0};
+  if ((st = check_cuda(cudaMemcpyAsync(tot, e->totals, sizeof(tot), cudaMemcpyDeviceToHost, s), "copy")) ||
+      (st = check_cuda(cudaStreamSynchronize(s), "sync")))
+    return st;
+  std::vector<uint8_t> flags(n_vecs), bws(n_vecs);
+  cudaMemcpy(flags.data(), e->sl.flags, n_vecs, cudaMemcpyDeviceToHost);
+  cudaMemcpy(bws.data(), e->sl.bw, n_vecs, cudaMemcpyDeviceToHost);
+  size_t fb = 0, rd = 0, bwsum = 0;
+  for (size_t i = 0; i < n_vecs; ++i) {
+    fb += flags[i] & 1;
+    rd += (flags[i] >> 1) & 1;
+    bwsum += bws[i];
+  }
+  std::memset(out, 0, sizeof(*out));
+  flsgpu_alp_column &c = out->column;
+  c.n_values = n_values;
+  c.ffor.n_values = n_values;
+  c.ffor.bp.n_values = n_values;
+  c.ffor.bp.n_vecs = n_vecs;
+  c.ffor.bp.packed_array = e->packed;
+  c.ffor.bp.bit_widths = e->sl.bw;
+  c.ffor.bp.vector_offsets = e->off_words;
+  c.ffor.bases = e->sl.base;
+  c.factor_indices = e->sl.fac;
+  c.fraction_indices = e->sl.exp;
+  c.n_exceptions = tot[1];
+  c.exceptions_offsets = e->off_exc;
+  c.exceptions = e->exc;
+  c.positions = e->pos;
+  c.counts = e->sl.count;
+  out->n_packed_words = tot[0];
+  out->n_exceptions = tot[1];
+  // reference accounting (alp-bindings.cu:19-43): packed bytes + 10 B per
+  // exception + 3 + 8 B of per-vector overhead
+  out->compressed_bytes = tot[0] * 8 + tot[1] * 10 + n_vecs * 11;
+  out->n_fallback = fb;
+  out->n_rd = rd;
+  out->mean_bit_width = n_vecs ? (double)bwsum / (double)n_vecs : 0.0;
+  return FLSGPU_OK;
+}
+
+}  // extern "C"

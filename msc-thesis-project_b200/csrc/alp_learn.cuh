@@ -1,0 +1,71 @@
+// alp_learn.cuh -- shared definitions of the GPU ALP encoder and the learned
+// (exponent, factor) proposal network.
+#pragma once
+
+#include <cuda_bf16.h>
+
+#include "common.cuh"
+#include "../../include/flsgpu_b200_ext.h"
+
+namespace flsb200 {
+
+// Classes: the 190 (exponent e, factor f) pairs with 0 <= f <= e <= 18
+// (encoder.hpp:166-167 iterates them), numbered e*(e+1)/2 + f; class 190
+// stands for ALP-RD; class 191 pads the output layer to 192.
+constexpr int kClassRD = 190;
+constexpr int kClasses = 191;
+constexpr int kOut = 192;
+constexpr int kFeatures = 64;
+constexpr int kHidden = 128;
+
+__host__ __device__ constexpr int pair_class(int e, int f) { return e * (e + 1) / 2 + f; }
+__host__ __device__ inline int class_exp(int c) {
+  int e = 0;
+  while ((e + 1) * (e + 2) / 2 <= c) ++e;
+  return e;
+}
+__host__ __device__ inline int class_fac(int c) {
+  const int e = class_exp(c);
+  return c - e * (e + 1) / 2;
+}
+
+// Per-vector encode results in fixed slots (1024 entries per vector), before
+// compaction into the contiguous column.
+struct EncodeSlots {
+  uint64_t *packed;   // n_vecs * 1024 words
+  double *exc;        // n_vecs * 1024
+  uint16_t *pos;      // n_vecs * 1024
+  uint8_t *bw;
+  uint64_t *base;
+  uint8_t *fac;
+  uint8_t *exp;
+  uint16_t *count;
+  uint8_t *flags;     // 1 = the proposal fell back to the plain search
+};
+
+// Launchers (alp_encode.cu)
+flsgpu_status run_plain_labels(const double *vals, size_t n_vecs, int16_t *labels, int32_t *est,
+                               cudaStream_t s);
+// encode (mode 0: plain search; 1: verified proposals with fallback), then
+// scan of the per-vector sizes (totals[0] = packed words, totals[1] =
+// exceptions) and compaction into packed / exc / pos
+flsgpu_status run_alp_encode(const double *vals, size_t n_vecs, int mode, const int16_t *cand,
+                             int k_cand, int max_exc, const EncodeSlots &sl, size_t *off_words,
+                             size_t *off_exc, size_t *totals, uint64_t *packed, double *exc,
+                             uint16_t *pos, cudaStream_t s);
+
+struct GemmArgs {
+  const __nv_bfloat16 *A;
+  const __nv_bfloat16 *B;
+  int lda, ldb;
+  int M, N, K;          // N <= 256; K % 16 == 0
+  float *Cf;            // optional fp32 output
+  __nv_bfloat16 *Cb;    // optional bf16 output
+  int ldc;
+  const float *bias;    // optional, per column
+  int relu;
+  uint32_t *status;     // 0x100: an mbarrier wait gave up
+};
+flsgpu_status gemm_tn(const GemmArgs &g, cudaStream_t s);
+
+}  // namespace flsb200

@@ -101,10 +101,12 @@ def lib() -> C.CDLL:
 
 
 def exported_symbols() -> list[str]:
-    """Entry points declared in include/flsgpu_b200.h."""
-    hdr = (PKG.parent / "include" / "flsgpu_b200.h").read_text()
+    """Entry points declared in include/*.h."""
     import re
-    return sorted(set(re.findall(r"\b(flsgpu_[a-z0-9_]+)\s*\(", hdr)))
+    names = set()
+    for hdr in sorted((PKG.parent / "include").glob("*.h")):
+        names |= set(re.findall(r"\b(flsgpu_[a-z0-9_]+)\s*\(", hdr.read_text()))
+    return sorted(names)
 
 
 def _check(status: int) -> None:
@@ -158,6 +160,13 @@ class DeviceColumn:
     @property
     def n_vecs(self) -> int:
         return (self.n_values + 1023) // 1024
+
+    @property
+    def device(self):
+        for t in self.buffers.values():
+            if hasattr(t, "device"):
+                return t.device
+        return _torch().device("cuda", _torch().cuda.current_device())
 
     def compressed_bytes(self) -> int:
         """Bytes a full decode reads: packed words, per-vector metadata and
@@ -254,7 +263,7 @@ def decompress(col: DeviceColumn, out=None, o: DecodeOpts | None = None, stream=
     torch = _torch()
     if out is None:
         out = torch.empty(col.n_values, dtype=getattr(torch, TORCH_OF_BITS[col.dtype]),
-                          device=col.buffers[next(iter(col.buffers))].device)
+                          device=col.device)
     f = _fn(f"flsgpu_decompress_{col.kind}_{col.dtype}")
     _check(f(C.byref(col.c), P(_ptr(out)), C.byref(o) if o is not None else None,
              P(_stream_handle(stream))))
@@ -265,7 +274,7 @@ def sum_(col: DeviceColumn, out=None, workspace=None, o: DecodeOpts | None = Non
     """Decode fused with a sum: u64 (mod 2^64) for integer columns, f64 with
     the fixed reduction tree for f64 ALP columns."""
     torch = _torch()
-    dev = col.buffers[next(iter(col.buffers))].device
+    dev = col.device
     if col.dtype in ("u32", "u64"):
         out = out if out is not None else torch.empty(1, dtype=torch.int64, device=dev)
         f = _fn(f"flsgpu_sum_{col.kind}_{col.dtype}")
@@ -287,7 +296,7 @@ _CT = {"u32": C.c_uint32, "u64": C.c_uint64, "f32": C.c_float, "f64": C.c_double
 
 def query(col: DeviceColumn, magic, found=None, o: DecodeOpts | None = None, stream=None):
     torch = _torch()
-    dev = col.buffers[next(iter(col.buffers))].device
+    dev = col.device
     if found is None:
         found = torch.zeros(1, dtype=torch.uint8, device=dev)
     f = _fn(f"flsgpu_query_{col.kind}_{col.dtype}")
@@ -298,7 +307,7 @@ def query(col: DeviceColumn, magic, found=None, o: DecodeOpts | None = None, str
 
 def compute(col: DeviceColumn, n_repetitions: int = 10, out=None, o=None, stream=None):
     torch = _torch()
-    dev = col.buffers[next(iter(col.buffers))].device
+    dev = col.device
     out = out if out is not None else torch.zeros(1, dtype=torch.uint8, device=dev)
     f = _fn(f"flsgpu_compute_{col.kind}_{col.dtype}")
     _check(f(C.byref(col.c), C.c_uint32(n_repetitions), P(_ptr(out)),
@@ -309,7 +318,7 @@ def compute(col: DeviceColumn, n_repetitions: int = 10, out=None, o=None, stream
 def query_multi_column(cols: Sequence[DeviceColumn], value, out=None, o=None, stream=None):
     torch = _torch()
     c0 = cols[0]
-    dev = c0.buffers[next(iter(c0.buffers))].device
+    dev = c0.device
     out = out if out is not None else torch.zeros(1, dtype=torch.uint8, device=dev)
     arr = (type(c0.c) * len(cols))(*[c.c for c in cols])
     f = _fn(f"flsgpu_query_multi_column_{c0.kind}_{c0.dtype}")
@@ -320,3 +329,228 @@ def query_multi_column(cols: Sequence[DeviceColumn], value, out=None, o=None, st
 
 def launch_count() -> int:
     return int(lib().flsgpu_launch_count())
+
+
+# ---------------------------------------------------------------------------
+# batched persistent decode and the fused pair query
+# ---------------------------------------------------------------------------
+TYPE_CODE = {"u32": 0, "u64": 1, "f32": 2, "f64": 3}
+ENCODING_CODE = {"bp": 0, "ffor": 1, "alp": 2, "alpx": 3}
+
+
+class BatchColumnC(C.Structure):
+    _fields_ = [("type", C.c_uint32), ("encoding", C.c_uint32), ("column", P), ("d_out", P)]
+
+
+class Batch:
+    """Many columns decoded by one persistent launch (or a replayed graph)."""
+
+    def __init__(self, cols: Sequence[DeviceColumn], outs, o: DecodeOpts | None = None):
+        self.cols = list(cols)
+        self.outs = list(outs)
+        arr = (BatchColumnC * len(cols))()
+        for i, (c, out) in enumerate(zip(cols, outs)):
+            arr[i] = BatchColumnC(TYPE_CODE[c.dtype], ENCODING_CODE[c.kind],
+                                  C.cast(C.pointer(c.c), P), _ptr(out))
+        self._arr = arr
+        h = P()
+        _check(_fn("flsgpu_batch_create")(arr, SZ(len(cols)), C.byref(o) if o is not None else None,
+                                         C.byref(h)))
+        self.h = h
+
+    def decompress(self, stream=None):
+        _check(_fn("flsgpu_batch_decompress")(self.h, P(_stream_handle(stream))))
+
+    def decompress_each(self, sync_each: bool = False, stream=None):
+        _check(_fn("flsgpu_batch_decompress_each")(self.h, C.c_int(int(sync_each)),
+                                                  P(_stream_handle(stream))))
+
+    def capture(self, stream=None):
+        _check(_fn("flsgpu_batch_capture_graph")(self.h, P(_stream_handle(stream))))
+
+    def replay(self, stream=None):
+        _check(_fn("flsgpu_batch_replay")(self.h, P(_stream_handle(stream))))
+
+    def total_vectors(self) -> int:
+        f = lib().flsgpu_batch_total_vectors
+        f.restype = SZ
+        f.argtypes = [P]
+        return int(f(self.h))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            f = lib().flsgpu_batch_destroy
+            f.restype = None
+            f.argtypes = [P]
+            f(self.h)
+            self.h = None
+
+
+class PairQuery:
+    """For each (A f64 ALP, B u32 FFOR) pair: sum(A where B < median(B))."""
+
+    def __init__(self, a_cols: Sequence[DeviceColumn], b_cols: Sequence[DeviceColumn], device):
+        torch = _torch()
+        n = len(a_cols)
+        self.a_cols, self.b_cols = list(a_cols), list(b_cols)
+        self.results = torch.zeros(max(n, 1), dtype=torch.float64, device=device)
+        self.medians = torch.zeros(max(n, 1), dtype=torch.int32, device=device)
+        self.status = torch.zeros(1, dtype=torch.int32, device=device)
+        aa = (ALPColumnC * max(n, 1))(*[c.c for c in a_cols])
+        bb = (FFORColumnC * max(n, 1))(*[c.c for c in b_cols])
+        h = P()
+        _check(_fn("flsgpu_pair_query_create")(aa, bb, SZ(n), P(_ptr(self.results)),
+                                              P(_ptr(self.medians)), P(_ptr(self.status)),
+                                              C.byref(h)))
+        self.h = h
+
+    def run(self, stream=None):
+        _check(_fn("flsgpu_pair_query_run")(self.h, P(_stream_handle(stream))))
+
+    def capture(self, stream=None):
+        _check(_fn("flsgpu_pair_query_capture_graph")(self.h, P(_stream_handle(stream))))
+
+    def replay(self, stream=None):
+        _check(_fn("flsgpu_pair_query_replay")(self.h, P(_stream_handle(stream))))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            f = lib().flsgpu_pair_query_destroy
+            f.restype = None
+            f.argtypes = [P]
+            f(self.h)
+            self.h = None
+
+
+# ---------------------------------------------------------------------------
+# GPU ALP encoder with the learned proposal, and the tensor-core GEMM
+# ---------------------------------------------------------------------------
+class EncodeResultC(C.Structure):
+    _fields_ = [("column", ALPColumnC), ("n_packed_words", SZ), ("n_exceptions", SZ),
+                ("compressed_bytes", SZ), ("n_fallback", SZ), ("n_rd", SZ),
+                ("mean_bit_width", C.c_double)]
+
+
+class AlpEncoder:
+    """GPU ALP encoder for f64 columns; mode 0 = plain per-vector search,
+    mode 1 = learned proposal verified on samples, with fallback."""
+
+    def __init__(self, seed: int = 1):
+        h = P()
+        _check(_fn("flsgpu_alp_encoder_create")(C.c_uint32(seed), C.byref(h)))
+        self.h = h
+
+    def train(self, values, epochs=8, batch=1024, lr=2e-3, stream=None):
+        lf, ll = C.c_float(), C.c_float()
+        _check(_fn("flsgpu_alp_encoder_train")(self.h, P(_ptr(values)), SZ(values.numel()),
+                                              C.c_uint32(epochs), C.c_uint32(batch),
+                                              C.c_float(lr), C.byref(lf), C.byref(ll),
+                                              P(_stream_handle(stream))))
+        return lf.value, ll.value
+
+    def encode(self, values, mode: int, stream=None) -> EncodeResultC:
+        r = EncodeResultC()
+        _check(_fn("flsgpu_alp_encode_f64")(self.h, P(_ptr(values)), SZ(values.numel()),
+                                           C.c_uint32(mode), C.byref(r),
+                                           P(_stream_handle(stream))))
+        return r
+
+    def propose(self, values, k=3, stream=None):
+        torch = _torch()
+        cand = torch.empty(values.numel() // 1024 * k, dtype=torch.int16, device=values.device)
+        _check(_fn("flsgpu_alp_encoder_propose")(self.h, P(_ptr(values)), SZ(values.numel()),
+                                                C.c_uint32(k), P(_ptr(cand)),
+                                                P(_stream_handle(stream))))
+        return cand.view(-1, k)
+
+    def params(self) -> np.ndarray:
+        f = lib().flsgpu_alp_encoder_param_count
+        f.restype = SZ
+        out = np.zeros(int(f()), np.float32)
+        _check(_fn("flsgpu_alp_encoder_get_params")(self.h, out.ctypes.data_as(P)))
+        return out
+
+    def set_params(self, p: np.ndarray):
+        p = np.ascontiguousarray(p, np.float32)
+        _check(_fn("flsgpu_alp_encoder_set_params")(self.h, p.ctypes.data_as(P)))
+
+    def gradients(self, features, labels, stream=None):
+        torch = _torch()
+        f = lib().flsgpu_alp_encoder_param_count
+        f.restype = SZ
+        g = torch.empty(int(f()), dtype=torch.float32, device=features.device)
+        loss = C.c_float()
+        _check(_fn("flsgpu_alp_encoder_gradients")(self.h, P(_ptr(features)), P(_ptr(labels)),
+                                                  C.c_uint32(labels.numel()), P(_ptr(g)),
+                                                  C.byref(loss), P(_stream_handle(stream))))
+        return g, loss.value
+
+    def save(self, path: str):
+        _check(_fn("flsgpu_alp_encoder_save")(self.h, str(path).encode()))
+
+    def load(self, path: str):
+        _check(_fn("flsgpu_alp_encoder_load")(self.h, str(path).encode()))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            f = lib().flsgpu_alp_encoder_destroy
+            f.restype = None
+            f.argtypes = [P]
+            f(self.h)
+            self.h = None
+
+
+def encoded_column(res: EncodeResultC, n_values: int, keep=None) -> DeviceColumn:
+    """The encoder's output as a decodable DeviceColumn (device arrays owned
+    by the encoder; valid until its next encode)."""
+    return DeviceColumn("alp", "f64", n_values, res.column, {"_owner": keep} if keep else {},
+                        int(res.n_packed_words))
+
+
+def plain_labels(values, stream=None):
+    torch = _torch()
+    n = values.numel() // 1024
+    lab = torch.empty(n, dtype=torch.int16, device=values.device)
+    est = torch.empty(n, dtype=torch.int32, device=values.device)
+    _check(_fn("flsgpu_alp_plain_labels")(P(_ptr(values)), SZ(values.numel()), P(_ptr(lab)),
+                                         P(_ptr(est)), P(_stream_handle(stream))))
+    return lab, est
+
+
+def alp_features(values, stream=None):
+    torch = _torch()
+    out = torch.empty(values.numel() // 1024, 64, dtype=torch.bfloat16, device=values.device)
+    _check(_fn("flsgpu_alp_features")(P(_ptr(values)), SZ(values.numel()), P(_ptr(out)),
+                                     P(_stream_handle(stream))))
+    return out
+
+
+def gemm_bf16_tn(A, B, bias=None, relu=False, status=None, stream=None):
+    """C = A @ B.T (+bias)(relu) on the tensor cores; A [M,K], B [N,K] bf16."""
+    torch = _torch()
+    M, K = A.shape
+    N = B.shape[0]
+    Cf = torch.empty(M, N, dtype=torch.float32, device=A.device)
+    _check(_fn("flsgpu_gemm_bf16_tn")(P(_ptr(A)), C.c_int(A.stride(0)), P(_ptr(B)),
+                                     C.c_int(B.stride(0)), C.c_int(M), C.c_int(N), C.c_int(K),
+                                     P(_ptr(Cf)), None, C.c_int(N), P(_ptr(bias)),
+                                     C.c_int(int(relu)), P(_ptr(status)),
+                                     P(_stream_handle(stream))))
+    return Cf
+
+
+class _CudaArray:
+    def __init__(self, ptr: int, n: int, typestr: str):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": typestr,
+                                         "data": (int(ptr), False), "version": 2}
+
+
+def device_array(ptr: int, n: int, dtype):
+    """A torch view of n elements of raw device memory (no copy)."""
+    torch = _torch()
+    typestr = np.dtype(dtype).str
+    if n == 0:
+        return torch.empty(0, dtype=getattr(torch, {"<u8": "int64", "<f8": "float64", "|u1": "uint8",
+                                                      "<u2": "int16", "<u4": "int32"}.get(typestr, "uint8")),
+                           device="cuda")
+    return torch.as_tensor(_CudaArray(ptr, n, typestr), device="cuda")

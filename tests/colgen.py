@@ -112,3 +112,21 @@ def alp_values(seed: int, n_vecs: int, f64: bool, dmax: int, exc_rate: float = 0
     v = vals.view(ut).copy()
     v[m] = pat
     return v.view(dt)
+
+
+def learned_values(seed: int, n_vecs: int) -> np.ndarray:
+    """Value-level f64 columns of the learned-proposal benchmark shape: per
+    vector d in {0..6} decimal digits, scale 10^k (k in 0..8), Gaussian or
+    uniform magnitude; 10% of the vectors are full-mantissa noise."""
+    rng = np.random.default_rng(seed)
+    d = rng.integers(0, 7, n_vecs)
+    k = rng.integers(0, 9, n_vecs)
+    gauss = rng.random(n_vecs) < 0.5
+    noise = rng.random(n_vecs) < 0.1
+    m = np.where(np.repeat(gauss, 1024), rng.standard_normal(n_vecs * 1024),
+                 rng.uniform(-1.0, 1.0, n_vecs * 1024))
+    scale = 10.0 ** np.repeat(k, 1024)
+    dd = 10.0 ** np.repeat(d, 1024)
+    vals = np.round(m * scale * dd) / dd
+    vals = np.where(np.repeat(noise, 1024), m * scale, vals)
+    return vals.astype(np.float64)

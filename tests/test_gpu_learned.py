@@ -1,0 +1,169 @@
+"""The GPU ALP encoder and the learned (exponent, factor) proposal:
+  * the tcgen05 BF16 GEMM against a torch fp32 reference of the same op;
+  * the network's gradients against the numpy oracle (oracle/mlp_oracle.py);
+  * the plain per-vector search against the oracle's search, label for label;
+  * encode -> decode exactness and byte parity of the packed words with the
+    oracle's encoder for the same (exponent, factor);
+  * training reduces the loss, and the learned encoder keeps the compression
+    ratio within 1% of the plain search while decoding bit-exactly, where the
+    method without the network (the reference's rowgroup sampling) loses
+    far more."""
+import numpy as np
+import pytest
+
+import colgen
+import flsgpu_b200 as F
+from oracle import binding as B
+from oracle import mlp_oracle
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("M,N,K", [(128, 128, 64), (300, 192, 128), (64, 64, 16), (256, 128, 4096),
+                                   (1000, 256, 192)])
+def test_tcgen05_gemm_matches_torch_fp32(cuda, M, N, K):
+    import torch
+    g = torch.Generator(device=cuda).manual_seed(M + N + K)
+    A = (torch.randn(M, K, device=cuda, generator=g)).to(torch.bfloat16)
+    Bm = (torch.randn(N, K, device=cuda, generator=g)).to(torch.bfloat16)
+    bias = torch.randn(N, device=cuda, generator=g)
+    status = torch.zeros(1, dtype=torch.int32, device=cuda)
+    for relu in (False, True):
+        C = F.gemm_bf16_tn(A, Bm, bias=bias, relu=relu, status=status)
+        ref = A.float() @ Bm.float().T + bias
+        if relu:
+            ref = torch.relu(ref)
+        torch.testing.assert_close(C, ref, rtol=1e-4, atol=1e-3 * K ** 0.5)
+    assert int(status.item()) == 0
+
+
+def test_gradients_match_numpy_oracle(cuda):
+    import torch
+    enc = F.AlpEncoder(seed=3)
+    params = enc.params()
+    rng = np.random.default_rng(0)
+    rows = 256
+    feats = torch.tensor(rng.uniform(-1, 1, (rows, 64)), dtype=torch.float32).to(torch.bfloat16)
+    labels = torch.tensor(rng.integers(0, 191, rows), dtype=torch.int16)
+    g, loss = enc.gradients(feats.to(cuda), labels.to(cuda))
+    want_loss, want = mlp_oracle.forward_backward(params, feats.float().numpy(),
+                                                  labels.numpy().astype(np.int64))
+    got = g.cpu().numpy().astype(np.float64)
+    assert abs(loss - want_loss) < 1e-3 * max(1.0, abs(want_loss))
+    err = np.linalg.norm(got - want) / np.linalg.norm(want)
+    assert err < 2e-2, err
+    # per parameter block
+    sizes = [64 * 128, 128, 128 * 128, 128, 192 * 128, 192]
+    o = 0
+    for n in sizes:
+        a, b = got[o:o + n], want[o:o + n]
+        if np.linalg.norm(b) > 0:
+            assert np.linalg.norm(a - b) / np.linalg.norm(b) < 3e-2
+        o += n
+
+
+def _oracle_label(vec):
+    r = B.oracle().orc_alp_vector_best_f64(B.ptr(np.ascontiguousarray(vec)), None)
+    if r < 0:
+        return 190
+    e, f = r // 32, r % 32
+    return e * (e + 1) // 2 + f
+
+
+def test_plain_search_labels_match_oracle(cuda):
+    import torch
+    vals = colgen.learned_values(11, 600)
+    lab, _ = F.plain_labels(torch.from_numpy(vals).to(cuda))
+    lab = lab.cpu().numpy()
+    want = np.array([_oracle_label(vals[i * 1024:(i + 1) * 1024]) for i in range(600)])
+    assert np.array_equal(lab, want)
+
+
+def _pair_of(cls):
+    e = 0
+    while (e + 1) * (e + 2) // 2 <= cls:
+        e += 1
+    return e, cls - e * (e + 1) // 2
+
+
+def test_plain_encode_roundtrip_and_byte_parity(cuda):
+    import torch
+    n_vecs = 300
+    vals = colgen.learned_values(12, n_vecs)
+    vals[5 * 1024 + 7] = np.nan
+    vals[9 * 1024 + 3] = -0.0
+    vals[9 * 1024 + 4] = np.inf
+    d_vals = torch.from_numpy(vals).to(cuda)
+    enc = F.AlpEncoder(seed=1)
+    res = enc.encode(d_vals, 0)
+    col = F.encoded_column(res, vals.size, enc)
+    got = F.decompress(col).cpu().numpy().view(np.uint64)
+    assert np.array_equal(got, vals.view(np.uint64))
+    # pull the column back and check each vector against the oracle encoder
+    c = res.column
+    n_words, n_exc_total = int(res.n_packed_words), int(res.n_exceptions)
+    host = lambda ptr, n, dt: F.device_array(ptr, n, dt).cpu().numpy()  # noqa: E731
+    bw = host(c.ffor.bp.bit_widths, n_vecs, np.uint8)
+    offs = host(c.ffor.bp.vector_offsets, n_vecs, np.uint64)
+    base = host(c.ffor.bases, n_vecs, np.uint64)
+    fac = host(c.factor_indices, n_vecs, np.uint8)
+    exp = host(c.fraction_indices, n_vecs, np.uint8)
+    counts = host(c.counts, n_vecs, np.uint16)
+    eoffs = host(c.exceptions_offsets, n_vecs, np.uint64)
+    packed = host(c.ffor.bp.packed_array, n_words, np.uint64)
+    exc = host(c.exceptions, n_exc_total, np.float64)
+    pos = host(c.positions, n_exc_total, np.uint16)
+    o = B.oracle()
+    for i in range(n_vecs):
+        vec = np.ascontiguousarray(vals[i * 1024:(i + 1) * 1024])
+        cls = _oracle_label(vec)
+        if cls != 190:
+            assert (int(exp[i]), int(fac[i])) == _pair_of(cls), i
+        ints = np.zeros(1024, np.int64)
+        ex = np.zeros(1024, np.float64)
+        ps = np.zeros(1024, np.uint16)
+        n_exc = o.orc_alp_encode_vector_f64(B.ptr(vec), int(exp[i]), int(fac[i]), B.ptr(ints),
+                                            B.ptr(ex), B.ptr(ps))
+        assert n_exc == counts[i], i
+        assert np.array_equal(pos[int(eoffs[i]):int(eoffs[i]) + n_exc], ps[:n_exc])
+        assert np.array_equal(exc[int(eoffs[i]):int(eoffs[i]) + n_exc].view(np.uint64),
+                              ex[:n_exc].view(np.uint64))
+        mn = int(ints.min())
+        w = int(int(ints.max()) - mn).bit_length()
+        assert w == bw[i] and (mn & (2 ** 64 - 1)) == int(base[i]), i
+        buf = np.zeros(1024, np.uint64)
+        o.orc_ffor_u64(B.ptr(ints.view(np.uint64)), B.ptr(buf), w, mn & (2 ** 64 - 1))
+        assert np.array_equal(packed[int(offs[i]):int(offs[i]) + 16 * w], buf[:16 * w]), i
+
+
+def test_training_and_learned_encoder(cuda, tmp_path):
+    import torch
+    train = torch.from_numpy(colgen.learned_values(21, 16384)).to(cuda)
+    test = colgen.learned_values(22, 2048)
+    d_test = torch.from_numpy(test).to(cuda)
+    enc = F.AlpEncoder(seed=5)
+    l0, l1 = enc.train(train, epochs=12, batch=1024, lr=3e-3)
+    assert l1 < 0.5 * l0
+    plain = enc.encode(d_test, 0)
+    plain_bytes = plain.compressed_bytes
+    learned = enc.encode(d_test, 1)
+    learned_bytes = learned.compressed_bytes
+    # decode is exact for the learned encoder's column too
+    col = F.encoded_column(learned, test.size, enc)
+    got = F.decompress(col).cpu().numpy().view(np.uint64)
+    assert np.array_equal(got, test.view(np.uint64))
+    ratio_plain = test.nbytes / plain_bytes
+    ratio_learned = test.nbytes / learned_bytes
+    assert ratio_learned >= 0.99 * ratio_plain, (ratio_learned, ratio_plain)
+    # the network's proposals are accepted for most vectors
+    assert learned.n_fallback < 0.4 * 2048
+    # the method without the network: the reference's rowgroup sampling
+    ref = B.alp_encode(test, rowgroup_vecs=100)
+    if ref is not None:
+        assert ratio_learned > test.nbytes / ref["compressed_bytes"]
+    # save / load round trip
+    p = tmp_path / "net.bin"
+    enc.save(str(p))
+    enc2 = F.AlpEncoder(seed=9)
+    enc2.load(str(p))
+    assert np.array_equal(enc.params(), enc2.params())
