@@ -142,10 +142,11 @@ def max_over_ranks(x: float, world: int) -> float:
 # ---------------------------------------------------------------------------
 # workload: FFOR at scale
 # ---------------------------------------------------------------------------
-def make_ffor_columns(scale: float, dev):
+def make_ffor_columns(scale: float, dev, only=None):
     """One u32 column of 2^28 * scale values per width 0..32, one u64 column
     of 2^27 * scale values per width 0..64; random packed words (so every
-    value is uniform in [0, 2^w)), random bases."""
+    value is uniform in [0, 2^w)), random bases.  `only`: a set of
+    (bits, width) to build, for profiling one column."""
     import torch
     import flsgpu_b200 as F
     cols = []
@@ -156,6 +157,8 @@ def make_ffor_columns(scale: float, dev):
         n_vecs = n_values // 1024
         nl = 1024 // bits
         for w in range(bits + 1):
+            if only is not None and (bits, w) not in only:
+                continue
             n_words = n_vecs * w * nl
             packed = torch.randint(-2 ** 31, 2 ** 31, (max(n_words, 1) * (bits // 32),),
                                    dtype=torch.int32, device=dev, generator=g)
@@ -187,7 +190,10 @@ def run_ffor(args, rank, world, dev):
     import torch
     import flsgpu_b200 as F
 
-    cols = make_ffor_columns(args.scale, dev)
+    only = None
+    if args.only:
+        only = {(int(t.split(":")[0][1:]), int(t.split(":")[1])) for t in args.only.split(",")}
+    cols = make_ffor_columns(args.scale, dev, only)
     out = torch.empty(max(c.n_values for _, _, c in cols) * 8 // 4, dtype=torch.int32, device=dev)
     total_read = sum(col_bytes(c)[0] for _, _, c in cols)
     total_write = sum(col_bytes(c)[1] for _, _, c in cols)
@@ -380,6 +386,26 @@ def run_batch(args, dev):
 # ---------------------------------------------------------------------------
 # workload: learned ALP parameter proposal vs the plain search (GPU encoder)
 # ---------------------------------------------------------------------------
+def learned_values(seed: int, n_vecs: int):
+    """f64 columns of the learned-proposal shape: per vector d in {0..6}
+    decimal digits, scale 10^k (k in 0..8), Gaussian or uniform magnitude;
+    10% of the vectors are full-mantissa noise.  The same generator as the
+    test suite's, so the network trained here sees the tests' distribution."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    d = rng.integers(0, 7, n_vecs)
+    k = rng.integers(0, 9, n_vecs)
+    gauss = rng.random(n_vecs) < 0.5
+    noise = rng.random(n_vecs) < 0.1
+    m = np.where(np.repeat(gauss, 1024), rng.standard_normal(n_vecs * 1024),
+                 rng.uniform(-1.0, 1.0, n_vecs * 1024))
+    scale = 10.0 ** np.repeat(k, 1024)
+    dd = 10.0 ** np.repeat(d, 1024)
+    vals = np.round(m * scale * dd) / dd
+    vals = np.where(np.repeat(noise, 1024), m * scale, vals)
+    return vals.astype(np.float64)
+
+
 def run_learned(args, dev):
     """Trains the proposal network on one synthetic column (2^24 values) and
     encodes a second one of 2^26 values (the learned-proposal benchmark
@@ -387,12 +413,11 @@ def run_learned(args, dev):
     uniform magnitude, 10% full-mantissa noise vectors) with the plain
     per-vector search and with the network's proposals."""
     import torch
-    import colgen
     import flsgpu_b200 as F
     stream = torch.cuda.current_stream()
     n_eval = int(2 ** 26 * args.scale) // 1024 * 1024
-    train = torch.from_numpy(colgen.learned_values(101, max(1024, int(2 ** 24 * args.scale) // 1024))).to(dev)
-    evals = torch.from_numpy(colgen.learned_values(202, n_eval // 1024)).to(dev)
+    train = torch.from_numpy(learned_values(101, max(1024, int(2 ** 24 * args.scale) // 1024))).to(dev)
+    evals = torch.from_numpy(learned_values(202, n_eval // 1024)).to(dev)
     enc = F.AlpEncoder(seed=7)
     t0 = time.perf_counter()
     l0, l1 = enc.train(train, epochs=args.epochs, batch=1024, lr=3e-3)
@@ -422,12 +447,14 @@ def run_learned(args, dev):
     ms_search = ev_time(lambda: F.plain_labels(evals))
     ms_propose = ev_time(lambda: enc.propose(evals, 3))
     in_bytes = evals.numel() * 8
-    # the reference's CPU encoder on a bounded sample (rowgroup sampling
-    # search, one state per rowgroup of 100 vectors as upstream ALP)
+    # the reference's CPU encoder (oracle restatement, one thread) on the
+    # same column: rowgroup sampling search, one state per rowgroup of 100
+    # vectors as upstream ALP; rowgroups it would send to ALP-RD stay on
+    # their ALP top-k so that the column is comparable
     from oracle import binding as B
-    sample = colgen.learned_values(202, 512)
+    sample = evals.cpu().numpy()
     t = time.perf_counter()
-    ref_col = B.alp_encode(sample, rowgroup_vecs=100)
+    ref_col = B.alp_encode(sample, rowgroup_vecs=100, rd_as_alp=True)
     ref_s = time.perf_counter() - t
     return dict(ms_plain=ms_plain, ms_learned=ms_learned, ms_search=ms_search,
                 ms_propose=ms_propose, in_bytes=in_bytes, plain_bytes=plain_bytes,
@@ -575,6 +602,8 @@ def main():
                     help="fraction of the benchmark column sizes (1.0 = full)")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--only", default="",
+                    help="ffor workload: columns to build, e.g. u32:6,u64:20 (profiling)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -637,8 +666,9 @@ def main():
                 "cpu_baseline": {"value": round(r["ref_gbs"], 3) if r["ref_gbs"] else None,
                                  "unit": "GB/s", "cores": 1, "kind": "port",
                                  "ratio": round(r["ref_ratio"], 4) if r["ref_ratio"] else None,
-                                 "sample": "512 vectors, oracle restatement of alp::encode with "
-                                           "rowgroup sampling (100 vectors per state)"}}))
+                                 "sample": "the whole evaluation column, oracle restatement of "
+                                           "alp::encode with rowgroup sampling (100 vectors per "
+                                           "state, ALP-RD rowgroups kept on ALP)"}}))
         return
     if args.workload == "batch":
         r = run_batch(args, dev)

@@ -287,10 +287,11 @@ __global__ void __launch_bounds__(256)
     int bw;
     int n_exc = encode_vector(vec, e, f, t, sl.packed + v * VEC, sl.exc + v * VEC,
                               sl.pos + v * VEC, &base, &bw);
-    // Fall back when the proposal leaves more than max_exc exceptions; ALP-RD
-    // vectors (per the network) are encoded with its best ALP pair and not
-    // searched again.
-    if (mode == 1 && !fallback && !rd_net && n_exc > max_exc) {
+    // Fall back when the proposal leaves more than max_exc exceptions, ALP-RD
+    // proposals included: their ALP pair is then the plain search's, so the
+    // column's size never depends on how far the network's ALP candidates
+    // are from the search's choice on high-exception vectors.
+    if (mode == 1 && !fallback && n_exc > max_exc) {
       // the proposal leaves too many exceptions: plain search and re-encode
       __syncwarp();
       fallback = true;

@@ -70,6 +70,7 @@ _ORACLE_SIGS = {
     "orc_alp_encode_f32": (I, [P, SZ, SZ] + [P] * 10 + [P]),
     "orc_alp_rowgroup_topk_f64": (I, [P, SZ, P, P]),
     "orc_alp_rowgroup_topk_f32": (I, [P, SZ, P, P]),
+    "orc_set_rd_as_alp": (None, [I]),
     "orc_alp_vector_best_f64": (I, [P, P]),
     "orc_alp_vector_choose_f64": (None, [P, I, P, P, P, P]),
     "orc_alp_encode_vector_f64": (I, [P, I, I, P, P, P]),
@@ -172,11 +173,13 @@ def pack(values: np.ndarray, bw: int, bits: int, lib=None) -> np.ndarray:
     return out[: bw * (1024 // bits)].copy()
 
 
-def alp_encode(values: np.ndarray, rowgroup_vecs: int = 100):
+def alp_encode(values: np.ndarray, rowgroup_vecs: int = 100, rd_as_alp: bool = False):
     """Oracle ALP encode of a whole column (n % 1024 == 0).  Returns a dict of
     arrays in the reference's host::ALPColumn layout, or None when sampling
-    selects ALP-RD."""
+    selects ALP-RD for a rowgroup (as alp::encode throws).  With rd_as_alp
+    such rowgroups keep their ALP top-k instead (an ALP-only encoder)."""
     lib = oracle()
+    lib.orc_set_rd_as_alp(1 if rd_as_alp else 0)
     f64 = values.dtype == np.float64
     ut = np.uint64 if f64 else np.uint32
     n_vecs = values.size // 1024

@@ -357,6 +357,14 @@ static int combo_better(const combo_t *a, const combo_t *b) {
 }
 
 /* find_top_k_combinations, encoder.hpp:134-230 (generic over PT). */
+/* When set, a rowgroup whose best sampled estimate reaches the ALP-RD limit
+ * keeps its ALP top-k instead of being rejected (encoder.hpp:208-211 switches
+ * such a rowgroup to ALP-RD, which alp::encode turns into an
+ * EncodingException, alp-bindings.cu:76-79).  Used to time and size the
+ * rowgroup search as an ALP-only encoder on data with ALP-RD rowgroups. */
+static int g_rd_as_alp = 0;
+void orc_set_rd_as_alp(int on) { g_rd_as_alp = on; }
+
 #define DEFINE_TOPK(SUF, PT, ST, UT, MAXE, EXCBITS, RDLIM, CB)               \
   static int topk_from_sample_##SUF(const PT *smp, size_t n_smp,            \
                                     uint8_t *k_exp, uint8_t *k_fac,         \
@@ -414,7 +422,7 @@ static int combo_better(const combo_t *a, const combo_t *b) {
       off += ss;                                                            \
     }                                                                       \
     if (best_out) *best_out = best;                                         \
-    if (best >= RDLIM) return -1;                                           \
+    if (best >= RDLIM && !g_rd_as_alp) return -1;                          \
     /* selection sort with the reference's strict total order */            \
     for (int i = 0; i < n_combos; ++i)                                      \
       for (int j = i + 1; j < n_combos; ++j)                                \

@@ -108,6 +108,9 @@ int orc_alp_rowgroup_topk_f64(const double *rowgroup, size_t n_values,
                               uint8_t *k_exp, uint8_t *k_fac);
 int orc_alp_rowgroup_topk_f32(const float *rowgroup, size_t n_values,
                               uint8_t *k_exp, uint8_t *k_fac);
+/* 1: rowgroups at the ALP-RD limit keep their ALP top-k (ALP-only encoder);
+ * 0 (default): they are rejected as alp::encode rejects them. */
+void orc_set_rd_as_alp(int on);
 /* Per-vector exhaustive search: top-k restricted to one vector's 32
  * samples (every 32nd value).  Returns the packed label e*32+f, or -1 when
  * no pair has >= 2 non-exceptions or the estimate crosses the RD limit.

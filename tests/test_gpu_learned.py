@@ -146,6 +146,9 @@ def test_training_and_learned_encoder(cuda, tmp_path):
     assert l1 < 0.5 * l0
     plain = enc.encode(d_test, 0)
     plain_bytes = plain.compressed_bytes
+    # per-vector exception counts of the plain column (the workspace is
+    # reused by the next encode)
+    counts = F.device_array(plain.column.counts, 2048, np.uint16).cpu().numpy()
     learned = enc.encode(d_test, 1)
     learned_bytes = learned.compressed_bytes
     # decode is exact for the learned encoder's column too
@@ -155,12 +158,18 @@ def test_training_and_learned_encoder(cuda, tmp_path):
     ratio_plain = test.nbytes / plain_bytes
     ratio_learned = test.nbytes / learned_bytes
     assert ratio_learned >= 0.99 * ratio_plain, (ratio_learned, ratio_plain)
-    # the network's proposals are accepted for most vectors
-    assert learned.n_fallback < 0.4 * 2048
+    # The plain search is the fallback whenever the proposal leaves more than
+    # 3% exceptions (30 of 1024).  On this data many vectors exceed that under
+    # the plain search's own pair (ALP-RD territory, and decimals whose
+    # decode by FRAC[e] rounds differently), so they fall back whatever the
+    # proposal; the network adds at most 10% of the vectors on top.
+    inherent = int((counts > 30).sum())
+    assert learned.n_fallback <= inherent + 0.1 * 2048, (learned.n_fallback, inherent)
     # the method without the network: the reference's rowgroup sampling
-    ref = B.alp_encode(test, rowgroup_vecs=100)
-    if ref is not None:
-        assert ratio_learned > test.nbytes / ref["compressed_bytes"]
+    # search (rowgroups of 100 vectors), kept on ALP where it would pick RD
+    ref = B.alp_encode(test, rowgroup_vecs=100, rd_as_alp=True)
+    assert ref is not None
+    assert ratio_learned > 1.2 * (test.nbytes / ref["compressed_bytes"])
     # save / load round trip
     p = tmp_path / "net.bin"
     enc.save(str(p))
