@@ -107,6 +107,27 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # distributed plumbing (replicas)
 # ---------------------------------------------------------------------------
+def profiled_traffic(name: str, alg_bytes_per_launch: float):
+    """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum)
+    of the dominant kernel, from the committed ncu summary `profiles/<name>`,
+    scaled to this run's launch size by algorithmic bytes (the capture shows
+    traffic proportional to them).  None when the summary is absent."""
+    p = Path(__file__).resolve().parent / "profiles" / name
+    try:
+        txt = p.read_text()
+    except OSError:
+        return None
+    vals = {}
+    for line in txt.splitlines():
+        k, _, v = line.strip().partition(":")
+        if k in ("traffic_bytes_per_launch", "algorithmic_bytes_per_launch"):
+            vals[k] = float(v)
+    if len(vals) != 2:
+        return None
+    return round(vals["traffic_bytes_per_launch"] / vals["algorithmic_bytes_per_launch"]
+                 * alg_bytes_per_launch)
+
+
 def dist_init():
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -722,8 +743,11 @@ def main():
             "roofline": {"bound": "hbm", "achieved": round(res["achieved"], 1),
                          "peak": hbm, "unit": "GB/s", "frac": round(res["achieved"] / hbm, 4),
                          "peak_kind": pk_kind,
-                         "kernel": "k_column<FFOR, STORE> (flsgpu_decompress_ffor_u32/u64)",
-                         "traffic": None},
+                         "kernel": "k_store<T> (flsgpu_decompress_ffor_u32/u64)",
+                         "algorithmic_bytes_per_launch": round(res["bytes_step"] / res["n_columns"]),
+                         "traffic": profiled_traffic("k_store_ffor_at_scale.md",
+                                                     res["bytes_step"] / res["n_columns"]),
+                         "traffic_source": "profiles/k_store_ffor_at_scale.md (ncu, one pass)"},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": res["launches"],
             "clocks": res["clocks"],
         }
