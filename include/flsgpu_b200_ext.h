@@ -81,8 +81,9 @@ void flsgpu_pair_query_destroy(flsgpu_pair_query *q);
  * samples, estimate and tie rules of encoder.hpp:134-230); mode 1 asks the
  * network for its three best pairs, chooses among them with the reference's
  * second-level rule (encoder.hpp:237-300) and falls back to the plain search
- * when the choice leaves more than 30 exceptions (3%) in the vector or the
- * network proposes ALP-RD.  Exceptions store the original values, so the
+ * when the choice leaves more than 30 exceptions (3%) in the vector (a
+ * vector whose top proposal is ALP-RD is encoded with its best proposed ALP
+ * pair under the same rule).  Exceptions store the original values, so the
  * column decodes exactly either way.  The network: 64 features of the 32
  * samples -> 128 -> 128 -> 192 logits (190 pairs, ALP-RD, padding), BF16
  * weights, FP32 accumulation on the tensor cores (tcgen05), trained on the
