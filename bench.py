@@ -276,6 +276,172 @@ def run_ffor(args, rank, world, dev):
 
 
 # ---------------------------------------------------------------------------
+# workload: ALP / ALP-RD decode at scale
+# ---------------------------------------------------------------------------
+def make_alp_columns(scale: float, dev, seed: int = 31):
+    """The ALP / ALP-RD decode configuration, generated on the device:
+    * f64 ALP, 2^27 values: integers uniform in [-10^6, 10^6] divided by
+      10^d (d uniform per vector in 0..4), 1% of positions replaced by random
+      non-NaN 64-bit patterns; encoded by the library's GPU encoder (plain
+      per-vector search);
+    * f64 ALP-RD, 2^27 values uniform in [0, 1) with full mantissa: cut at
+      52 bits (right part = mantissa, left part = exponent), dictionary of the
+      8 most frequent exponents, other exponents as exceptions, both parts
+      packed by the GPU packer (BP);
+    * f32 ALP, 2^28 values: integers uniform in [-10^6, 10^6] times
+      FRAC[d] (d uniform per vector in 0..3, factor 0: the value ALP decodes
+      them to), FFOR-packed at the signed minimum by the GPU packer, 1% of
+      positions replaced by random non-NaN 32-bit patterns as exceptions.
+    Returns [(name, column, expected values, read bytes, written bytes)]."""
+    import torch
+    import flsgpu_b200 as F
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    out = []
+
+    def exc_layout(mask, nv):
+        counts = mask.view(nv, 1024).sum(1)
+        offs = torch.zeros(nv, dtype=torch.int64, device=dev)
+        offs[1:] = torch.cumsum(counts, 0)[:-1]
+        flat = torch.nonzero(mask).squeeze(1)
+        return counts.to(torch.int16), offs, flat, (flat % 1024).to(torch.int16)
+
+    # f64 ALP, value level, GPU encoder
+    n = int(2 ** 27 * scale) // 1024 * 1024
+    nv = n // 1024
+    ints = torch.randint(-10 ** 6, 10 ** 6 + 1, (n,), dtype=torch.int64, device=dev, generator=g)
+    p10 = torch.tensor([1.0, 10.0, 100.0, 1000.0, 10000.0], dtype=torch.float64, device=dev)
+    d = torch.randint(0, 5, (nv,), device=dev, generator=g).repeat_interleave(1024)
+    vals = ints.double() / p10[d]
+    m = torch.rand(n, device=dev, generator=g) < 0.01
+    pat = torch.randint(-2 ** 63, 2 ** 63 - 1, (n,), dtype=torch.int64, device=dev, generator=g)
+    pat = torch.where(torch.isnan(pat.view(torch.float64)), pat & ~(1 << 62), pat)
+    vals.view(torch.int64)[m] = pat[m]
+    del ints, d, m, pat
+    enc = F.AlpEncoder(seed=1)
+    res = enc.encode(vals, 0)
+    col = F.encoded_column(res, n, enc)
+    col.buffers["_enc"] = enc
+    rd_b = int(res.n_packed_words) * 8 + nv * 29 + int(res.n_exceptions) * 10
+    out.append(("alp_f64", col, vals, rd_b, n * 8))
+
+    # f64 ALP-RD
+    vals = torch.rand(n, dtype=torch.float64, device=dev, generator=g)
+    bits = vals.view(torch.int64)
+    left = bits >> 52
+    right = bits & ((1 << 52) - 1)
+    cnt = torch.bincount(left, minlength=2048)
+    top = torch.argsort(cnt, descending=True, stable=True)[:8]
+    lut = torch.full((2048,), -1, dtype=torch.int64, device=dev)
+    lut[top] = torch.arange(8, device=dev)
+    idx = lut[left]
+    mask = idx < 0
+    counts, eoffs, flat, pos = exc_layout(mask, nv)
+    exc = left[flat].to(torch.int16)
+    rcol = F.ffor_encode(right, F.BASE_ZERO)
+    assert int(rcol.buffers["bit_widths"].min()) == 52 and int(rcol.buffers["bit_widths"].max()) == 52
+    lbuf = F.ffor_encode(idx.clamp(min=0).to(torch.int16), F.BASE_ZERO)
+    dicts = top.to(torch.int16)
+    dict_idx = torch.zeros(nv, dtype=torch.int32, device=dev)
+    left_c = F.BPColumnC(n, nv, lbuf["_keep"].data_ptr(), lbuf["bit_widths"].data_ptr(),
+                         lbuf["vector_offsets"].data_ptr())
+    n_exc = int(flat.numel())
+    c = F.ALPRDColumnC(n, rcol.c, left_c, dicts.data_ptr(), dict_idx.data_ptr(), n_exc,
+                       eoffs.data_ptr(), exc.data_ptr() if n_exc else 0,
+                       pos.data_ptr() if n_exc else 0, counts.data_ptr())
+    keep = {"right": rcol, "left": lbuf, "dicts": dicts, "dict_idx": dict_idx, "exc": exc,
+            "pos": pos, "counts": counts, "eoffs": eoffs}
+    col = F.DeviceColumn("alprd", "f64", n, c, {"_keep": keep}, rcol.n_packed)
+    rd_b = rcol.n_packed * 8 + lbuf["n_packed"] * 2 + nv * 32 + 16 + n_exc * 4
+    out.append(("alprd_f64", col, vals, rd_b, n * 8))
+    del bits, left, right, idx, mask, lut
+
+    # f32 ALP, compressed level with the values ALP decodes to
+    n = int(2 ** 28 * scale) // 1024 * 1024
+    nv = n // 1024
+    ints = torch.randint(-10 ** 6, 10 ** 6 + 1, (n,), dtype=torch.int32, device=dev, generator=g)
+    frac = torch.tensor([1.0, 0.1, 0.01, 0.001], dtype=torch.float32, device=dev)
+    dv = torch.randint(0, 4, (nv,), device=dev, generator=g)
+    vals = ints.float() * frac[dv.repeat_interleave(1024)]
+    m = torch.rand(n, device=dev, generator=g) < 0.01
+    pat = torch.randint(-2 ** 31, 2 ** 31 - 1, (n,), dtype=torch.int32, device=dev, generator=g)
+    pat = torch.where(torch.isnan(pat.view(torch.float32)), pat & ~(1 << 30), pat)
+    vals.view(torch.int32)[m] = pat[m]
+    counts, eoffs, flat, pos = exc_layout(m, nv)
+    exc = vals[flat].contiguous()
+    fcol = F.ffor_encode(ints, F.BASE_SIGNED_MIN)
+    fac = torch.zeros(nv, dtype=torch.uint8, device=dev)
+    fr = dv.to(torch.uint8)
+    n_exc = int(flat.numel())
+    c = F.ALPColumnC(n, fcol.c, None, None, fac.data_ptr(), fr.data_ptr(), n_exc,
+                     eoffs.data_ptr(), exc.data_ptr(), pos.data_ptr(), counts.data_ptr())
+    keep = {"ffor": fcol, "fac": fac, "fr": fr, "exc": exc, "pos": pos, "counts": counts,
+            "eoffs": eoffs}
+    col = F.DeviceColumn("alp", "f32", n, c, {"_keep": keep}, fcol.n_packed)
+    rd_b = fcol.n_packed * 4 + nv * 25 + n_exc * 6
+    out.append(("alp_f32", col, vals, rd_b, n * 4))
+    del ints, m, pat
+    return out
+
+
+def run_alp(args, rank, world, dev):
+    import torch
+    import flsgpu_b200 as F
+    t0 = time.perf_counter()
+    cols = make_alp_columns(args.scale, dev)
+    gen_s = time.perf_counter() - t0
+    stream = torch.cuda.current_stream()
+    outs = [torch.empty_like(v) for _, _, v, _, _ in cols]
+    exact = {}
+    for (name, c, v, _, _), o in zip(cols, outs):
+        F.decompress(c, out=o, stream=stream)
+        ib = torch.int64 if v.element_size() == 8 else torch.int32
+        exact[name] = bool(torch.equal(o.view(ib), v.view(ib)))
+
+    def step(events=None):
+        for i, ((name, c, v, _, _), o) in enumerate(zip(cols, outs)):
+            if events is not None:
+                events[i][0].record(stream)
+            F.decompress(c, out=o, stream=stream)
+            if events is not None:
+                events[i][1].record(stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    events = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in cols] for _ in range(args.steps)]
+    launches0 = F.launch_count()
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for st in range(args.steps):
+            step(events[st])
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    launches = F.launch_count() - launches0
+    ms = max_over_ranks(e0.elapsed_time(e1), world)
+    per = {}
+    kern_ms = 0.0
+    for i, (name, c, v, rb, wb) in enumerate(cols):
+        t = statistics.mean(events[st][i][0].elapsed_time(events[st][i][1])
+                            for st in range(args.steps))
+        kern_ms += t
+        per[name] = {"gbs": round((rb + wb) / (t / 1e3) / 1e9, 1), "ms": round(t, 4),
+                     "read_bytes": rb, "write_bytes": wb, "bit_exact": exact[name],
+                     "values": c.n_values}
+    bytes_step = sum(rb + wb for _, _, _, rb, wb in cols)
+    return dict(gbs=bytes_step * args.steps * world / (ms / 1e3) / 1e9, ms=ms,
+                bytes_step=bytes_step, per=per, achieved=bytes_step / (kern_ms / 1e3) / 1e9,
+                launches=launches, clocks=clk.summary(), gen_s=gen_s,
+                exact=all(exact.values()))
+
+
+# ---------------------------------------------------------------------------
 # workload: batched uneven decode + fused pair query
 # ---------------------------------------------------------------------------
 def make_batch_columns(n_cols: int, dev, seed: int = 4):
@@ -616,7 +782,10 @@ def main():
     ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--workload", choices=["ffor", "ffor-sum", "batch", "learned"], default="ffor")
+    ap.add_argument("--workload", choices=["ffor", "ffor-sum", "alp", "batch", "learned",
+                                           "autotune"], default="ffor")
+    ap.add_argument("--tune", action="store_true",
+                    help="run the decode autotuner (flsgpu_b200.autotune) before measuring")
     ap.add_argument("--epochs", type=int, default=12, help="learned workload: training epochs")
     ap.add_argument("--columns", type=int, default=2000, help="batch workload: column count")
     ap.add_argument("--scale", type=float, default=1.0,
@@ -690,6 +859,51 @@ def main():
                                  "sample": "the whole evaluation column, oracle restatement of "
                                            "alp::encode with rowgroup sampling (100 vectors per "
                                            "state, ALP-RD rowgroups kept on ALP)"}}))
+        return
+    if args.tune or args.workload == "autotune":
+        import flsgpu_b200 as F
+        t0 = time.perf_counter()
+        tuned = F.autotune()
+        tune_s = time.perf_counter() - t0
+        if args.workload == "autotune":
+            if rank == 0:
+                tab = tuned["table"]
+                print(json.dumps({
+                    "metric": "decode autotuner: per-width L2 prefetch and kernel variant",
+                    "value": round(tune_s, 2), "unit": "s", "n_gpus": world,
+                    "higher_is_better": False, "data": "synthetic",
+                    "table": {"variant": {f"{k[0]}/{k[1]}": v for k, v in tab["variant"].items()},
+                              "prefetch": {str(k): v for k, v in tab["prefetch"].items()}},
+                    "report": tuned["report"],
+                    "header": F.tuning_header(tab)}))
+            return
+    if args.workload == "alp":
+        r = run_alp(args, rank, world, dev)
+        pk, pk_kind = peaks()
+        hbm = float(pk["hbm_gbs"])
+        if rank == 0:
+            print(json.dumps({
+                "metric": "ALP / ALP-RD decode GB/s (compressed read + decoded write), 1 B200",
+                "value": round(r["gbs"], 1), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": round(r["ms"] / args.steps, 3),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64/f32", "data": "synthetic",
+                "config": {"workload": "ALP/ALP-RD decode: f64 ALP 2^27 values (d 0..4, 1% "
+                                       "exceptions), f64 ALP-RD 2^27 uniform [0,1), f32 ALP 2^28 "
+                                       "values (d 0..3, 1% exceptions)",
+                           "scale": args.scale,
+                           "l2": "every column's output (1 GiB) exceeds L2; no flush",
+                           "parallelism": f"replicas x{args.gpus}"},
+                "per_column": r["per"], "bit_exact": r["exact"],
+                "hbm_fraction": {"of_measured": round(r["gbs"] / world / hbm, 4),
+                                 "of_spec_8tbs": round(r["gbs"] / world / 8000.0, 4)},
+                "roofline": {"bound": "hbm", "achieved": round(r["achieved"], 1), "peak": hbm,
+                             "unit": "GB/s", "frac": round(r["achieved"] / hbm, 4),
+                             "peak_kind": pk_kind,
+                             "kernel": "k_store<f64/f32, ALP> and k_alprd<f64>",
+                             "traffic": None},
+                "gpu_launches": r["launches"], "clocks": r["clocks"],
+                "generation_s": round(r["gen_s"], 1)}))
         return
     if args.workload == "batch":
         r = run_batch(args, dev)

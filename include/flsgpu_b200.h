@@ -82,12 +82,16 @@ typedef enum flsgpu_patcher {
   FLSGPU_PATCHER_COUNT
 } flsgpu_patcher;
 
-/* B200 kernel variants (what an unpacker enum selects). */
+/* B200 kernel variants of the full decompression (no reference
+ * counterpart: the reference picks an unpacker per launch, this library a
+ * register budget).  Both decode every width with the same unpackers. */
 typedef enum flsgpu_variant {
-  FLSGPU_VARIANT_AUTO = 0,      /* autotuned table (flsgpu_autotune) */
-  FLSGPU_VARIANT_DIRECT = 1,    /* coalesced per-line register loads */
-  FLSGPU_VARIANT_STAGED = 2,    /* bulk-async (TMA) copy of each vector's
-                                   packed words into shared memory */
+  FLSGPU_VARIANT_AUTO = 0,       /* the tuned choice for the column's value
+                                    type and kind (flsgpu_tuning_*) */
+  FLSGPU_VARIANT_REGS = 1,       /* register-rich: 2 resident blocks per SM
+                                    for 32-bit lanes, 1 for 64-bit lanes */
+  FLSGPU_VARIANT_OCCUPANCY = 2,  /* register-capped for twice the resident
+                                    blocks (more loads in flight) */
   FLSGPU_VARIANT_COUNT
 } flsgpu_variant;
 
@@ -197,6 +201,34 @@ flsgpu_status flsgpu_decompress_alprd_f32(const flsgpu_alprd_column *column, flo
                                           const flsgpu_decode_opts *opts, flsgpu_stream stream);
 flsgpu_status flsgpu_decompress_alprd_f64(const flsgpu_alprd_column *column, double *d_out,
                                           const flsgpu_decode_opts *opts, flsgpu_stream stream);
+
+/* ---- FastLanes packing, the encoder side (fls::ffor src/fls/ffor.cpp:
+ *      29861, fls::pack src/fls/pack.cpp:29731, base / width rule of
+ *      analyze_ffor src/alp/encoder.hpp:104-115; the reference packs on the
+ *      CPU, vector by vector).  n_values % 1024 == 0.  Per vector: the base
+ *      (base_mode FLSGPU_BASE_MIN: unsigned minimum; FLSGPU_BASE_SIGNED_MIN:
+ *      minimum as a signed integer, as analyze_ffor; FLSGPU_BASE_ZERO: 0,
+ *      i.e. BP, d_bases may be NULL), the width bits(max - base), and the
+ *      packed words at d_vector_offsets[v] (exclusive prefix of width x
+ *      lanes).  d_packed must hold n_values elements (the widest case);
+ *      d_n_packed (optional, device) receives the number of packed words.
+ *      Output decodes with flsgpu_decompress_{ffor,bp}_* and is word for
+ *      word what fls::ffor / fls::pack write. ---- */
+#define FLSGPU_BASE_MIN 0u
+#define FLSGPU_BASE_SIGNED_MIN 1u
+#define FLSGPU_BASE_ZERO 2u
+flsgpu_status flsgpu_ffor_encode_u16(const uint16_t *d_values, size_t n_values, uint32_t base_mode,
+                                     uint16_t *d_packed, uint8_t *d_bit_widths,
+                                     uint64_t *d_vector_offsets, uint16_t *d_bases,
+                                     uint64_t *d_n_packed, flsgpu_stream stream);
+flsgpu_status flsgpu_ffor_encode_u32(const uint32_t *d_values, size_t n_values, uint32_t base_mode,
+                                     uint32_t *d_packed, uint8_t *d_bit_widths,
+                                     uint64_t *d_vector_offsets, uint32_t *d_bases,
+                                     uint64_t *d_n_packed, flsgpu_stream stream);
+flsgpu_status flsgpu_ffor_encode_u64(const uint64_t *d_values, size_t n_values, uint32_t base_mode,
+                                     uint64_t *d_packed, uint8_t *d_bit_widths,
+                                     uint64_t *d_vector_offsets, uint64_t *d_bases,
+                                     uint64_t *d_n_packed, flsgpu_stream stream);
 
 /* ---- decode fused with a sum (model: kernels::device::query_column,
  *      kernels.cuh:34-54).  Integer sums are exact mod 2^64.  Float sums

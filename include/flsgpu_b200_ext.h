@@ -56,6 +56,22 @@ flsgpu_status flsgpu_batch_decompress_each(flsgpu_batch *batch, int sync_each,
 size_t flsgpu_batch_total_vectors(const flsgpu_batch *batch);
 void flsgpu_batch_destroy(flsgpu_batch *batch);
 
+/* ---- decode tuning (no reference counterpart; the reference fixes its
+ *      unpacker per build in the generated bindings) ----------------------
+ * Process-wide state read at every launch: the kernel variant that
+ * FLSGPU_VARIANT_AUTO selects per value type (0 u32, 1 u64, 2 f32, 3 f64)
+ * and column kind (0 BP, 1 FFOR, 2 ALP, 3 ALP extended), and per lane width
+ * (32 or 64) a bit mask over bit widths 0..127: bit w asks the decode to
+ * prefetch the next vector's packed lines into L2 when that vector has
+ * width w.  Defaults are compiled in (autotune_table.h); the autotuner
+ * (flsgpu_b200.autotune) measures the variants on the device and installs
+ * its choice here.  Not synchronised with launches in flight: set it before
+ * decoding. */
+flsgpu_status flsgpu_tuning_set_variant(uint32_t type, uint32_t kind, uint32_t variant);
+flsgpu_status flsgpu_tuning_get_variant(uint32_t type, uint32_t kind, uint32_t *variant);
+flsgpu_status flsgpu_tuning_set_prefetch(uint32_t lane_bits, const uint64_t mask[2]);
+flsgpu_status flsgpu_tuning_get_prefetch(uint32_t lane_bits, uint64_t mask[2]);
+
 /* ---- fused pair query over compressed columns (no reference counterpart)
  * For each pair i: d_results[i] = sum of A_i[k] over positions k with
  * B_i[k] < median(B_i), where A_i is an f64 ALP column, B_i a u32 FFOR

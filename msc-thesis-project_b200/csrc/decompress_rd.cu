@@ -34,8 +34,27 @@ struct RDParams {
   void *out;
 };
 
+// Per-vector metadata, loaded two vectors ahead of its use.
+struct RDMeta {
+  size_t loff, roff, eo;
+  uint32_t di, cnt;
+  int rbw, lbw;
+};
+
+__device__ __forceinline__ RDMeta rd_meta(const RDParams &p, size_t vi) {
+  RDMeta m;
+  m.rbw = p.right_bw[vi];
+  m.lbw = p.left_bw[vi];
+  m.di = p.dict_index[vi];
+  m.loff = p.left_offs[vi];
+  m.roff = p.right_offs[vi];
+  m.cnt = p.counts[vi];
+  m.eo = p.exc_offs[vi];
+  return m;
+}
+
 template <typename T>
-__global__ void __launch_bounds__(256) k_alprd(const RDParams p) {
+__global__ void __launch_bounds__(256, sizeof(T) == 8 ? 2 : 1) k_alprd(const RDParams p) {
   using U = typename UintOf<T>::U;
   constexpr int MAXW = sizeof(U) * 8;
   __shared__ uint16_t s_left_all[8][VEC];
@@ -44,16 +63,35 @@ __global__ void __launch_bounds__(256) k_alprd(const RDParams p) {
   const size_t gw = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const size_t nw = ((size_t)gridDim.x * blockDim.x) >> 5;
   U *out_all = reinterpret_cast<U *>(p.out);
+  const U *right_all = reinterpret_cast<const U *>(p.right_packed);
 
+  RDMeta m0{}, m1{};
+  if (gw < p.n_vecs) {
+    m0 = rd_meta(p, gw);
+    if (m0.rbw <= MAXW) prefetch_packed(right_all + m0.roff, m0.rbw, t);
+  }
+  if (gw + nw < p.n_vecs) m1 = rd_meta(p, gw + nw);
   for (size_t vi = gw; vi < p.n_vecs; vi += nw) {
-    const int rbw = p.right_bw[vi], lbw = p.left_bw[vi];
-    if (rbw > MAXW || lbw > 16) {
+    const RDMeta m = m0;
+    // the next vector's right part is fetched into L2 while this one is
+    // decoded; metadata of the vector after it is in flight
+    if (vi + nw < p.n_vecs && m1.rbw <= MAXW) prefetch_packed(right_all + m1.roff, m1.rbw, t);
+    m0 = m1;
+    if (vi + 2 * nw < p.n_vecs) m1 = rd_meta(p, vi + 2 * nw);
+    if (m.rbw > MAXW || m.lbw > 16) {
       if (t == 0 && p.d_status) atomicOr(p.d_status, FLSGPU_BAD_BIT_WIDTH);
       continue;
     }
-    const uint16_t dct = (t < 8) ? p.dicts[8 * (size_t)p.dict_index[vi] + t] : 0;
-    const uint16_t *lin = p.left_packed + p.left_offs[vi];
-    switch_width16(lbw, [&](auto wc) {
+    const uint16_t dct = (t < 8) ? p.dicts[8 * (size_t)m.di + t] : 0;
+    // the first 32 exceptions, loaded with the left parts
+    uint32_t p0 = VEC;
+    uint16_t e0 = 0;
+    if ((uint32_t)t < m.cnt) {
+      p0 = p.pos[m.eo + t];
+      e0 = p.exc[m.eo + t];
+    }
+    const uint16_t *lin = p.left_packed + m.loff;
+    switch_width16(m.lbw, [&](auto wc) {
       constexpr int W = decltype(wc)::value;
       uint32_t wr[W > 0 ? W : 1];
       load_pair16<W>(lin, t, wr);
@@ -64,13 +102,12 @@ __global__ void __launch_bounds__(256) k_alprd(const RDParams p) {
       });
     });
     __syncwarp();
-    const uint32_t cnt = p.counts[vi];
-    const size_t eo = p.exc_offs[vi];
-    bool bad = false;
-    for (uint32_t i = t; i < cnt; i += 32) {
-      const uint32_t ps = p.pos[eo + i];
+    bool bad = (uint32_t)t < m.cnt && p0 >= VEC;
+    if (p0 < VEC) sl[p0] = e0;
+    for (uint32_t i = t + 32; i < m.cnt; i += 32) {
+      const uint32_t ps = p.pos[m.eo + i];
       if (ps < VEC)
-        sl[ps] = p.exc[eo + i];
+        sl[ps] = p.exc[m.eo + i];
       else
         bad = true;
     }
@@ -81,8 +118,9 @@ __global__ void __launch_bounds__(256) k_alprd(const RDParams p) {
     const size_t rem = p.n_values - vbase;
     const int lim = rem < (size_t)VEC ? (int)rem : VEC;
     U *out = out_all + vbase;
-    const U *rin = reinterpret_cast<const U *>(p.right_packed) + p.right_offs[vi];
+    const U *rin = right_all + m.roff;
     const XInt<U> ident{0};
+    const int rbw = m.rbw;
     decode_values<U>(rin, rbw, t, ident, [&](int idx, U r, auto...) {
       const U l = rbw >= MAXW ? U(0) : (U)((U)sl[idx] << rbw);
       if (idx < lim) out[idx] = l | r;

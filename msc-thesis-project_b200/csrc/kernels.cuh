@@ -53,6 +53,7 @@ struct KernelParams {
   uint64_t magic;          // bit pattern of the query value
   uint32_t n_rep;          // S_COMPUTE
   uint64_t runtime_zero;   // S_COMPUTE
+  uint64_t prefetch[2];    // bit w: L2-prefetch the next vector's packed lines when its width is w
 };
 
 // ---- value transforms (functors of the reference) ------------------------
@@ -104,6 +105,8 @@ template <typename T> struct Meta {
   U base;
   int w;
   int fi, ei;
+  uint32_t ecnt;  // ALPColumn: the vector's exception count (0 when not patched)
+  size_t eo;      // ALPColumn: index of its first exception
 };
 
 template <typename T, int KIND>
@@ -118,6 +121,14 @@ __device__ __forceinline__ Meta<T> load_meta(const ColumnParams &c, size_t vi) {
     m.ei = c.exp_idx[vi];
   } else {
     m.fi = m.ei = 0;
+  }
+  m.ecnt = 0;
+  m.eo = 0;
+  if constexpr (KIND == K_ALP) {
+    if (c.patch && c.counts) {
+      m.ecnt = c.counts[vi];
+      m.eo = c.exc_offs[vi];
+    }
   }
   return m;
 }
@@ -175,7 +186,6 @@ __device__ __forceinline__ void prefetch_packed(const void *vin, int w, int t) {
 // Decodes the calling thread's 32 values of a vector; put(idx, value) with
 // idx the position inside the vector, called in ascending value order.
 // Kernel variant bits (chosen per type and width by the autotuner):
-constexpr int VAR_PREFETCH = 1;  // metadata one vector ahead + L2 prefetch of packed lines
 constexpr int VAR_STCS = 2;      // streaming (evict-first) output stores
 constexpr int VAR_LD32 = 4;      // 64-bit lanes: 32-bit word loads (fewer live registers)
 constexpr int VAR_MINB2 = 8;     // register cap for two resident blocks per SM
@@ -184,23 +194,17 @@ constexpr int VAR_AUTO = 32;     // per-width policy from autotune_table.h
 constexpr int VAR_PAIR = 64;     // decode two same-width vectors per warp step (policy bit)
 constexpr int VAR_NOPAIR = 128;  // kernel variant: never pair
 constexpr int VAR_MINB4 = 256;   // kernel variant: 32-bit lanes capped for four blocks per SM
+constexpr int VAR_OCC = 512;     // kernel variant: registers capped for twice the resident blocks
 constexpr int VAR_DEFAULT = VAR_AUTO;
 
 // Policy bits in force for width W under kernel variant VAR.
+// The register-capped variant (VAR_OCC) decodes wide 64-bit half-lanes in
+// two runs of 16 values so that they fit its register budget.
 template <typename U, int VAR> __host__ __device__ constexpr int policy_of(int W) {
-  if constexpr ((VAR & VAR_AUTO) != 0) {
-    return sizeof(U) == 8 ? tuned::kPolicy64[W] : tuned::kPolicy32[W];
-  } else {
-    return VAR;
-  }
-}
-
-// Widths whose policy asks for an L2 prefetch of the next vector.
-template <typename U, int VAR> __host__ __device__ constexpr unsigned long long prefetch_mask() {
-  unsigned long long m = 0;
-  for (int w = 0; w <= (int)(sizeof(U) * 8) && w < 64; ++w)
-    if (policy_of<U, VAR>(w) & VAR_PREFETCH) m |= 1ull << w;
-  return m;
+  int pol = VAR;
+  if constexpr ((VAR & VAR_AUTO) != 0) pol = sizeof(U) == 8 ? tuned::kPolicy64[W] : tuned::kPolicy32[W];
+  if ((VAR & VAR_OCC) != 0 && sizeof(U) == 8 && W > 24) pol |= VAR_CHUNK;
+  return pol;
 }
 
 // Widths decoded two vectors at a time (both vectors' loads in flight before
@@ -330,7 +334,12 @@ template <typename T, int T_VAR> __device__ __forceinline__ void store_out(T *p,
 // loop is latency-bound at low widths, so occupancy matters more than
 // keeping every packed word of the widest cases in registers.
 template <typename T, int VAR> constexpr int min_blocks() {
-  return (VAR & VAR_MINB4) ? 4 : (VAR & VAR_MINB2) ? 2 : (sizeof(T) == 4 ? 2 : 1);
+  constexpr int base = sizeof(T) == 4 ? 2 : 1;
+  return (VAR & VAR_MINB4) ? 4 : (VAR & VAR_MINB2) ? 2 : (VAR & VAR_OCC) ? 2 * base : base;
+}
+
+__device__ __forceinline__ bool prefetch_width(const KernelParams &p, int w) {
+  return w < 128 && ((p.prefetch[w >> 6] >> (w & 63)) & 1);
 }
 
 // Decodes one vector into the output (row order), then patches its
@@ -350,6 +359,18 @@ __device__ __forceinline__ void store_one(const KernelParams &p, size_t vi, cons
   const size_t rem = c.n_values - vbase;
   const int lim = rem < (size_t)VEC ? (int)rem : VEC;
   T *out = reinterpret_cast<T *>(p.out) + vbase;
+  // ALPColumn: the vector's first 32 exceptions (position, value) are loaded
+  // before the decode, so their latency overlaps the packed words' instead
+  // of following the row stores.
+  [[maybe_unused]] uint32_t p0 = VEC;
+  [[maybe_unused]] T e0 = T(0);
+  [[maybe_unused]] const bool pre = KIND == K_ALP && c.patch && c.counts;
+  if constexpr (KIND == K_ALP) {
+    if (pre && (uint32_t)t < m.ecnt) {
+      p0 = c.pos[m.eo + t];
+      e0 = reinterpret_cast<const T *>(c.exc)[m.eo + t];
+    }
+  }
   if (lim == VEC) {
     decode_values<T, VAR>(vin, w, t, xf, [&](int idx, T v, auto pc) {
       store_out<T, decltype(pc)::value>(out + idx, v);
@@ -358,6 +379,24 @@ __device__ __forceinline__ void store_one(const KernelParams &p, size_t vi, cons
     decode_values<T, VAR>(vin, w, t, xf, [&](int idx, T v, auto pc) {
       if (idx < lim) store_out<T, decltype(pc)::value>(out + idx, v);
     });
+  }
+  if constexpr (KIND == K_ALP) {
+    if (pre) {
+      __syncwarp();
+      bool bad = (uint32_t)t < m.ecnt && p0 >= VEC;
+      if ((int)p0 < lim) out[p0] = e0;
+      const T *exc = reinterpret_cast<const T *>(c.exc);
+      for (uint32_t i = t + 32; i < m.ecnt; i += 32) {
+        const uint32_t ps = c.pos[m.eo + i];
+        if (ps < VEC) {
+          if ((int)ps < lim) out[ps] = exc[m.eo + i];
+        } else {
+          bad = true;
+        }
+      }
+      if (__any_sync(0xffffffffu, bad) && t == 0) flag_status(p.d_status, FLSGPU_BAD_EXCEPTION);
+      return;
+    }
   }
   if constexpr (IS_ALP) {
     if (c.patch) {
@@ -407,9 +446,9 @@ __global__ void __launch_bounds__(256, min_blocks<T, VAR>()) k_store(const Kerne
       hnb = vi + 2 * nw < n;
       if (hnb) nb = load_meta<T, KIND>(c, vi + 2 * nw);
     }
-    if constexpr ((VAR & VAR_PREFETCH) != 0) {
+    {
       const size_t vn = vi + (pair ? 2 : 1) * nw;
-      if (vn < n && na.w <= (int)(sizeof(U) * 8) && ((prefetch_mask<U, VAR>() >> na.w) & 1))
+      if (vn < n && na.w <= (int)(sizeof(U) * 8) && prefetch_width(p, na.w))
         prefetch_packed(reinterpret_cast<const U *>(c.packed) + na.off, na.w, t);
     }
     if (pair) {
@@ -473,15 +512,10 @@ __global__ void __launch_bounds__(256, min_blocks<T, VAR>()) k_column(const Kern
     int w;
     X xf;
     const Meta<T> cur = meta;
-    if constexpr ((VAR & VAR_PREFETCH) != 0) {
-      const size_t vn = vi + nw;
-      if (vn < c.n_vecs) {
-        meta = load_meta<T, KIND>(c, vn);
-        if (meta.w <= (int)(sizeof(U) * 8) && (prefetch_mask<U, VAR>() >> meta.w) & 1)
-          prefetch_packed(reinterpret_cast<const U *>(c.packed) + meta.off, meta.w, t);
-      }
-    } else if (vi + nw < c.n_vecs) {
+    if (vi + nw < c.n_vecs) {
       meta = load_meta<T, KIND>(c, vi + nw);
+      if (meta.w <= (int)(sizeof(U) * 8) && prefetch_width(p, meta.w))
+        prefetch_packed(reinterpret_cast<const U *>(c.packed) + meta.off, meta.w, t);
     }
     if (!setup_from_meta<T, KIND>(c, p.d_status, cur, t, vin, w, xf)) continue;
     const size_t vbase = vi * VEC;
@@ -598,19 +632,30 @@ static __global__ void __launch_bounds__(1024) k_pairwise_f64(const double *src,
 }
 
 // ---- host side ------------------------------------------------------------
+// Host-side decode tuning (capi.cu): the kernel variant used under
+// FLSGPU_VARIANT_AUTO per (value type, column kind), and the per-width L2
+// prefetch masks per lane width; defaults from autotune_table.h, replaced
+// by the autotuner through flsgpu_tuning_set_*.
+int tuned_variant(int type, int kind);
+void tuned_prefetch(int lane_bits, uint64_t out[2]);
+template <typename T> constexpr int type_code() {
+  return std::is_same<T, uint32_t>::value ? 0 : std::is_same<T, uint64_t>::value ? 1
+       : std::is_same<T, float>::value ? 2 : 3;
+}
+
 template <typename T, int KIND, int SINK> struct Launch {
   static constexpr bool STAGE = (KIND == K_ALP || KIND == K_ALPX) && SINK != S_STORE;
   static size_t smem() { return STAGE ? (size_t)8 * VEC * sizeof(T) : 0; }
-  static auto kernel() {
+  template <int V> static auto kernel() {
     if constexpr (SINK == S_STORE)
-      return k_store<T, KIND>;
+      return k_store<T, KIND, VAR_AUTO | V>;
     else
       return k_column<T, KIND, SINK>;
   }
-  static int blocks_per_sm() {
+  template <int V> static int blocks_per_sm() {
     static int bps = 0;
     if (bps == 0) {
-      auto kern = kernel();
+      auto kern = kernel<V>();
       if (smem() > 48 * 1024)
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem());
       int b = 0;
@@ -619,12 +664,22 @@ template <typename T, int KIND, int SINK> struct Launch {
     }
     return bps;
   }
-  static flsgpu_status run(const KernelParams &p, cudaStream_t s) {
-    if (p.c.n_vecs == 0) return FLSGPU_OK;
-    const unsigned grid = persistent_blocks(p.c.n_vecs, 8, blocks_per_sm());
-    kernel()<<<grid, 256, smem(), s>>>(p);
+  template <int V> static flsgpu_status launch(const KernelParams &p, cudaStream_t s) {
+    const unsigned grid = persistent_blocks(p.c.n_vecs, 8, blocks_per_sm<V>());
+    kernel<V>()<<<grid, 256, smem(), s>>>(p);
     note_launch();
-    return check_cuda(cudaGetLastError(), "k_column launch");
+    return check_cuda(cudaGetLastError(), "decode launch");
+  }
+  // variant: FLSGPU_VARIANT_* (full decompression only; the fused sinks
+  // have one kernel each)
+  static flsgpu_status run(KernelParams p, cudaStream_t s, uint32_t variant = FLSGPU_VARIANT_AUTO) {
+    if (p.c.n_vecs == 0) return FLSGPU_OK;
+    tuned_prefetch((int)sizeof(T) * 8, p.prefetch);
+    if constexpr (SINK == S_STORE) {
+      if (variant == FLSGPU_VARIANT_AUTO) variant = (uint32_t)tuned_variant(type_code<T>(), KIND);
+      if (variant == FLSGPU_VARIANT_OCCUPANCY) return launch<VAR_OCC>(p, s);
+    }
+    return launch<0>(p, s);
   }
 };
 
@@ -727,7 +782,8 @@ static flsgpu_status decompress(const Col *col, T *d_out, const flsgpu_decode_op
   if (!aligned<T>(d_out)) return set_error(FLSGPU_ERR_MISALIGNED, "output not aligned");
   p.d_status = o ? o->d_status : nullptr;
   p.out = d_out;
-  return Launch<T, KIND, S_STORE>::run(p, (cudaStream_t)stream);
+  return Launch<T, KIND, S_STORE>::run(p, (cudaStream_t)stream,
+                                       o ? o->variant : (uint32_t)FLSGPU_VARIANT_AUTO);
 }
 
 template <typename T, int KIND, typename Col>

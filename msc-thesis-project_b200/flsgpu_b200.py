@@ -41,7 +41,7 @@ UNPACKERS = ["Dummy", "OldFls", "SwitchCase", "Stateless", "StatelessBranchless"
              "StatefulBranchless"]
 PATCHERS = ["None", "Dummy", "Stateless", "Stateful", "Naive", "NaiveBranchless",
             "PrefetchPosition", "PrefetchAll", "PrefetchAllBranchless"]
-VARIANT_AUTO, VARIANT_DIRECT, VARIANT_STAGED = 0, 1, 2
+VARIANT_AUTO, VARIANT_REGS, VARIANT_OCCUPANCY = 0, 1, 2
 
 
 class FlsgpuError(RuntimeError):
@@ -191,6 +191,44 @@ def make_ffor_column(packed: np.ndarray, bit_widths: np.ndarray, offsets: np.nda
                         FFORColumnC(n_values, bp, _ptr(bufs["bases"])), bufs, packed.size)
 
 
+BASE_MIN, BASE_SIGNED_MIN, BASE_ZERO = 0, 1, 2
+
+
+def ffor_encode(values, base_mode: int = BASE_MIN, stream=None):
+    """FastLanes FFOR / BP packing on the GPU (flsgpu_ffor_encode_*) of a
+    device tensor of int16 / int32 / int64 (read as u16 / u32 / u64),
+    values.numel() % 1024 == 0.  Returns a DeviceColumn ("ffor", or "bp" for
+    BASE_ZERO) for 32- and 64-bit values, and a dict of the packed arrays for
+    16-bit values (ALP-RD left parts).  Synchronises to read the packed
+    size."""
+    torch = _torch()
+    n = values.numel()
+    bits = values.element_size() * 8
+    n_vecs = n // 1024
+    dev = values.device
+    packed = torch.empty(max(n, 1), dtype=values.dtype, device=dev)
+    bw = torch.empty(max(n_vecs, 1), dtype=torch.uint8, device=dev)
+    offs = torch.empty(max(n_vecs, 1), dtype=torch.int64, device=dev)
+    bases = torch.empty(max(n_vecs, 1), dtype=values.dtype, device=dev)
+    total = torch.zeros(1, dtype=torch.int64, device=dev)
+    f = _fn(f"flsgpu_ffor_encode_u{bits}")
+    _check(f(P(_ptr(values)), C.c_size_t(n), C.c_uint32(base_mode), P(_ptr(packed)),
+             P(_ptr(bw)), P(_ptr(offs)), P(_ptr(bases)), P(_ptr(total)),
+             P(_stream_handle(stream))))
+    n_packed = int(total.item())
+    bufs = {"packed": packed[:n_packed], "bit_widths": bw[:n_vecs], "vector_offsets": offs[:n_vecs],
+            "_keep": packed}
+    if bits == 16:
+        bufs["bases"] = bases[:n_vecs]
+        bufs["n_packed"] = n_packed
+        return bufs
+    bp = BPColumnC(n, n_vecs, _ptr(packed), _ptr(bw), _ptr(offs))
+    if base_mode == BASE_ZERO:
+        return DeviceColumn("bp", f"u{bits}", n, bp, bufs, n_packed)
+    bufs["bases"] = bases[:n_vecs]
+    return DeviceColumn("ffor", f"u{bits}", n, FFORColumnC(n, bp, _ptr(bases)), bufs, n_packed)
+
+
 def make_alp_column(col: dict, n_values: int, dtype, extended: bool = False,
                     device="cuda") -> DeviceColumn:
     """col: arrays in the reference's host::ALPColumn layout (as produced by
@@ -329,6 +367,201 @@ def query_multi_column(cols: Sequence[DeviceColumn], value, out=None, o=None, st
 
 def launch_count() -> int:
     return int(lib().flsgpu_launch_count())
+
+
+# ---------------------------------------------------------------------------
+# decode tuning and the autotuner
+# ---------------------------------------------------------------------------
+TYPE_CODES = {"u32": 0, "u64": 1, "f32": 2, "f64": 3}
+KIND_CODES = {"bp": 0, "ffor": 1, "alp": 2, "alpx": 3}
+
+
+def tuning_get() -> dict:
+    """The process-wide decode tuning: {"variant": {(type, kind): variant},
+    "prefetch": {lane_bits: sorted widths with L2 prefetch}}."""
+    out = {"variant": {}, "prefetch": {}}
+    v = C.c_uint32()
+    for tn, tc in TYPE_CODES.items():
+        for kn, kc in KIND_CODES.items():
+            _check(_fn("flsgpu_tuning_get_variant")(C.c_uint32(tc), C.c_uint32(kc), C.byref(v)))
+            out["variant"][(tn, kn)] = int(v.value)
+    for lb in (32, 64):
+        m = (C.c_uint64 * 2)()
+        _check(_fn("flsgpu_tuning_get_prefetch")(C.c_uint32(lb), m))
+        out["prefetch"][lb] = [w for w in range(lb + 1) if (m[w >> 6] >> (w & 63)) & 1]
+    return out
+
+
+def tuning_set(table: dict) -> None:
+    """Installs a table of the tuning_get() shape (entries may be missing)."""
+    for (tn, kn), var in table.get("variant", {}).items():
+        _check(_fn("flsgpu_tuning_set_variant")(C.c_uint32(TYPE_CODES[tn]),
+                                                C.c_uint32(KIND_CODES[kn]), C.c_uint32(var)))
+    for lb, widths in table.get("prefetch", {}).items():
+        m = (C.c_uint64 * 2)()
+        for w in widths:
+            m[w >> 6] |= 1 << (w & 63)
+        _check(_fn("flsgpu_tuning_set_prefetch")(C.c_uint32(int(lb)), m))
+
+
+def _synthetic_ffor(bits: int, w: int, n_values: int, g, dev) -> DeviceColumn:
+    """Random packed words at width w (every value uniform in [0, 2^w)),
+    random bases."""
+    torch = _torch()
+    n_vecs = n_values // 1024
+    nl = 1024 // bits
+    words = n_vecs * w * nl * (bits // 32)
+    packed = torch.randint(-2 ** 31, 2 ** 31, (max(words, 2),), dtype=torch.int32, device=dev,
+                           generator=g)
+    packed = packed.view(torch.int64) if bits == 64 else packed
+    bw = torch.full((n_vecs,), w, dtype=torch.uint8, device=dev)
+    offs = torch.arange(n_vecs, dtype=torch.int64, device=dev) * (w * nl)
+    bases = torch.randint(-2 ** 31, 2 ** 31, (n_vecs * (bits // 32),), dtype=torch.int32,
+                          device=dev, generator=g)
+    bases = bases.view(torch.int64) if bits == 64 else bases
+    bp = BPColumnC(n_values, n_vecs, packed.data_ptr(), bw.data_ptr(), offs.data_ptr())
+    return DeviceColumn("ffor", f"u{bits}", n_values, FFORColumnC(n_values, bp, bases.data_ptr()),
+                        {"packed": packed[:max(words // (bits // 32), 1)], "bit_widths": bw,
+                         "vector_offsets": offs, "bases": bases, "_keep": packed},
+                        words // (bits // 32))
+
+
+def _synthetic_alp(bits: int, w: int, n_values: int, exc_per_vec: int, g, dev) -> DeviceColumn:
+    """An ALP column over a synthetic FFOR part: bases 2..20, factor /
+    fraction indices in the lower half of their tables, exc_per_vec
+    exceptions per vector at distinct spread positions."""
+    torch = _torch()
+    f = _synthetic_ffor(bits, w, n_values, g, dev)
+    n_vecs = n_values // 1024
+    it = torch.int64 if bits == 64 else torch.int32
+    bases = torch.randint(2, 21, (n_vecs,), dtype=it, device=dev, generator=g)
+    f.buffers["bases"] = bases
+    f.c.bases = bases.data_ptr()
+    nf, ne = (19, 21) if bits == 64 else (10, 11)
+    fac = torch.randint(0, nf // 2 + 1, (n_vecs,), dtype=torch.uint8, device=dev, generator=g)
+    fr = torch.randint(0, ne // 2 + 1, (n_vecs,), dtype=torch.uint8, device=dev, generator=g)
+    k = exc_per_vec
+    counts = torch.full((n_vecs,), k, dtype=torch.int16, device=dev)
+    eoffs = torch.arange(n_vecs, dtype=torch.int64, device=dev) * k
+    stride = 1024 // max(k, 1)
+    shift = torch.randint(0, stride, (n_vecs, 1), device=dev, generator=g)
+    pos = ((torch.arange(k, device=dev).view(1, -1) * stride + shift) % 1024).to(torch.int16)
+    exc = torch.randn(max(n_vecs * k, 1), dtype=torch.float64 if bits == 64 else torch.float32,
+                      device=dev, generator=g)
+    pos = pos.reshape(-1) if k else torch.zeros(1, dtype=torch.int16, device=dev)
+    c = ALPColumnC(n_values, f.c, None, None, fac.data_ptr(), fr.data_ptr(), n_vecs * k,
+                   eoffs.data_ptr(), exc.data_ptr(), pos.data_ptr(), counts.data_ptr())
+    bufs = dict(f.buffers)
+    bufs.update({"factor_indices": fac, "fraction_indices": fr, "exceptions_offsets": eoffs,
+                 "exceptions": exc[:n_vecs * k], "positions": pos[:n_vecs * k], "counts": counts})
+    return DeviceColumn("alp", f"f{bits}", n_values, c, bufs, f.n_packed)
+
+
+def autotune(values_32: int = 2 ** 26, values_64: int = 2 ** 25, reps: int = 5, stream=None,
+             install: bool = True, alp_widths=None) -> dict:
+    """Measures the decode variants on the current device and picks, per
+    lane width and bit width, whether the decode prefetches the next
+    vector's packed lines into L2, and per value type and column kind the
+    kernel variant (register-rich or register-capped for occupancy).
+    Columns are synthetic (random packed words, every width of the lane
+    type; ALP columns at the given widths with 1% exceptions), each output
+    larger than L2.  Time per configuration: the best of `reps` launches
+    (CUDA events).  Returns the chosen table, the per-width GB/s of every
+    configuration and the gain over the compiled defaults; installs the
+    table unless install=False."""
+    torch = _torch()
+    dev = torch.device("cuda", torch.cuda.current_device())
+    g = torch.Generator(device=dev)
+    g.manual_seed(2024)
+    s = torch.cuda.current_stream() if stream is None else stream
+    before = tuning_get()
+
+    def best_ms(col, out, variant):
+        o = opts(variant=variant)
+        decompress(col, out=out, o=o, stream=s)
+        ts = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            decompress(col, out=out, o=o, stream=s)
+            e1.record(s)
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return min(ts)
+
+    def col_bytes(col):
+        bits = int(col.dtype[1:])
+        return col.compressed_bytes() + col.n_values * bits // 8
+
+    report = {"ffor": {}, "alp": {}}
+    table = {"variant": {}, "prefetch": {}}
+    variants = (VARIANT_REGS, VARIANT_OCCUPANCY)
+    for bits, n in ((32, values_32), (64, values_64)):
+        n -= n % 1024
+        out = torch.empty(n, dtype=torch.int32 if bits == 32 else torch.int64, device=dev)
+        per = {v: {} for v in variants}
+        for w in range(bits + 1):
+            col = _synthetic_ffor(bits, w, n, g, dev)
+            for pf in (False, True):
+                cur = tuning_get()["prefetch"][bits]
+                tuning_set({"prefetch": {bits: sorted(set(cur) | {w}) if pf
+                                         else [x for x in cur if x != w]}})
+                for v in variants:
+                    per[v][(w, pf)] = best_ms(col, out, v)
+            del col
+        totals = {v: sum(min(per[v][(w, False)], per[v][(w, True)]) for w in range(bits + 1))
+                  for v in variants}
+        var = min(variants, key=lambda v: totals[v])
+        pf_widths = [w for w in range(bits + 1) if per[var][(w, True)] < per[var][(w, False)]]
+        table["prefetch"][bits] = pf_widths
+        table["variant"][(f"u{bits}", "ffor")] = var
+        table["variant"][(f"u{bits}", "bp")] = var
+        tuning_set({"prefetch": {bits: pf_widths}})
+        nb = lambda w: (n * w // 8 + n // 1024 * (bits // 8 + 9) + n * bits // 8)  # noqa: E731
+        report["ffor"][f"u{bits}"] = {
+            "chosen_variant": var, "total_ms": {str(v): round(t, 4) for v, t in totals.items()},
+            "gbs": {str(v): [round(nb(w) / (min(per[v][(w, False)], per[v][(w, True)]) / 1e3) / 1e9, 1)
+                             for w in range(bits + 1)] for v in variants}}
+        del out
+    for bits, n in ((32, values_32), (64, values_64)):
+        n -= n % 1024
+        widths = alp_widths or ((8, 12, 16, 20, 24, 28) if bits == 32 else (8, 16, 20, 24, 32, 40, 48))
+        out = torch.empty(n, dtype=torch.float32 if bits == 32 else torch.float64, device=dev)
+        tot = {v: 0.0 for v in variants}
+        gbs = {v: [] for v in variants}
+        for w in widths:
+            col = _synthetic_alp(bits, w, n, 10, g, dev)
+            for v in variants:
+                t = best_ms(col, out, v)
+                tot[v] += t
+                gbs[v].append(round(col_bytes(col) / (t / 1e3) / 1e9, 1))
+            del col
+        var = min(variants, key=lambda v: tot[v])
+        table["variant"][(f"f{bits}", "alp")] = var
+        table["variant"][(f"f{bits}", "alpx")] = var
+        report["alp"][f"f{bits}"] = {"widths": list(widths), "chosen_variant": var,
+                                     "total_ms": {str(v): round(t, 4) for v, t in tot.items()},
+                                     "gbs": {str(v): g_ for v, g_ in gbs.items()}}
+        del out
+    if install:
+        tuning_set(table)
+    else:
+        tuning_set(before)
+    return {"table": table, "report": report, "defaults": before}
+
+
+def tuning_header(table: dict) -> str:
+    """The runtime part of a tuning table as the source of its compiled
+    defaults (kPrefetch32, kPrefetch64, kVariant in autotune_table.h)."""
+    def row(vals):
+        return ", ".join(f"{v:2d}" for v in vals)
+    p32 = [1 if w in table["prefetch"].get(32, []) else 0 for w in range(33)]
+    p64 = [1 if w in table["prefetch"].get(64, []) else 0 for w in range(65)]
+    var = [[table["variant"].get((tn, kn), VARIANT_REGS) for kn in KIND_CODES] for tn in TYPE_CODES]
+    return ("constexpr unsigned char kPrefetch32[33] = {" + row(p32) + "};\n"
+            "constexpr unsigned char kPrefetch64[65] = {" + row(p64) + "};\n"
+            "constexpr unsigned char kVariant[4][4] = {" +
+            ", ".join("{" + row(r) + "}" for r in var) + "};\n")
 
 
 # ---------------------------------------------------------------------------

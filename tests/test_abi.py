@@ -57,3 +57,24 @@ def test_multi_column_bounds():
     cols = (F.FFORColumnC * 17)()
     assert f(cols, C.c_uint32(17), C.c_uint32(0), C.c_void_p(16), None, None) == 1
     assert f(cols, C.c_uint32(0), C.c_uint32(0), C.c_void_p(16), None, None) == 1
+
+
+def test_decode_tuning_round_trip_and_checks():
+    """The tuning state is host-only: set / get round trip, bad arguments
+    rejected, the previous table restored."""
+    before = F.tuning_get()
+    try:
+        F.tuning_set({"variant": {("f64", "alp"): F.VARIANT_OCCUPANCY},
+                      "prefetch": {32: [3, 7, 32], 64: [0, 64]}})
+        t = F.tuning_get()
+        assert t["variant"][("f64", "alp")] == F.VARIANT_OCCUPANCY
+        assert t["prefetch"][32] == [3, 7, 32] and t["prefetch"][64] == [0, 64]
+        with pytest.raises(F.FlsgpuError):
+            F.tuning_set({"variant": {("u32", "ffor"): F.VARIANT_AUTO}})
+        with pytest.raises(F.FlsgpuError):
+            F._check(F._fn("flsgpu_tuning_set_prefetch")(16, None))
+    finally:
+        F.tuning_set(before)
+    assert F.tuning_get() == before
+    hdr = F.tuning_header(before)
+    assert "kPrefetch32[33]" in hdr and "kVariant[4][4]" in hdr

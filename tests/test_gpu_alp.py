@@ -22,27 +22,28 @@ def _dt(f64):
     return np.float64 if f64 else np.float32
 
 
-def _check(cuda, col, n_vecs, f64, extended=False, patcher=7):
+def _check(cuda, col, n_vecs, f64, extended=False, patcher=7, variant=F.VARIANT_AUTO):
     dt, ut = _dt(f64), _ut(f64)
     c = col
     if extended:
         c, _ = B.to_extended(col, n_vecs, dt)
     d = F.make_alp_column(c, n_vecs * 1024, dt, extended=extended, device=cuda)
-    got = F.decompress(d, o=F.opts(patcher=patcher)).cpu().numpy().view(ut)
+    got = F.decompress(d, o=F.opts(patcher=patcher, variant=variant)).cpu().numpy().view(ut)
     want = B.alp_decode(c, n_vecs, dt, extended=extended).view(ut)
     return got, want
 
 
 @pytest.mark.parametrize("f64", [True, False])
 @pytest.mark.parametrize("extended", [False, True])
-def test_alp_widths_and_exception_counts(cuda, f64, extended):
+@pytest.mark.parametrize("variant", [F.VARIANT_REGS, F.VARIANT_OCCUPANCY])
+def test_alp_widths_and_exception_counts(cuda, f64, extended, variant):
     bits = 64 if f64 else 32
-    for ec in [0, 1, 5, 10]:
+    for ec in [0, 1, 5, 10, 33, 70]:
         col = colgen.random_alp(1000 + ec, 64, f64, range(0, 17), [ec])
-        got, want = _check(cuda, col, 64, f64, extended)
+        got, want = _check(cuda, col, 64, f64, extended, variant=variant)
         assert np.array_equal(got, want), f"ec={ec}"
     col = colgen.random_alp(77, 256, f64, range(bits + 1), range(0, 40))
-    got, want = _check(cuda, col, 256, f64, extended)
+    got, want = _check(cuda, col, 256, f64, extended, variant=variant)
     assert np.array_equal(got, want)
 
 

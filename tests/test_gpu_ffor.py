@@ -43,7 +43,7 @@ def test_bp_every_width(cuda, bits):
 
 
 @pytest.mark.parametrize("bits", [32, 64])
-@pytest.mark.parametrize("variant", [F.VARIANT_AUTO, F.VARIANT_DIRECT, F.VARIANT_STAGED])
+@pytest.mark.parametrize("variant", [F.VARIANT_AUTO, F.VARIANT_REGS, F.VARIANT_OCCUPANCY])
 def test_ffor_mixed_widths(cuda, bits, variant):
     ut = np.uint64 if bits == 64 else np.uint32
     c = colgen.random_ffor(7 + bits, 3000, bits, range(bits + 1))
