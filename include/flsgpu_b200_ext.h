@@ -20,7 +20,8 @@ extern "C" {
  * Columns are grouped by value type; within a group all vectors of all
  * columns form one index space that a persistent grid takes in chunks from
  * an atomic counter, so a batch of columns of uneven length, type and bit
- * width decodes in one launch per value type present (at most four).  The
+ * width decodes in one launch per value type present (ALP and ALP-extended
+ * float columns in separate launches; at most six).  The
  * decode per vector is the single-column kernels' (same per-width autotuned
  * unpackers). */
 typedef enum flsgpu_type {
@@ -42,7 +43,9 @@ typedef struct flsgpu_batch flsgpu_batch;
  * The descriptors' device arrays must outlive the batch. */
 flsgpu_status flsgpu_batch_create(const flsgpu_batch_column *columns, size_t n_columns,
                                   const flsgpu_decode_opts *opts, flsgpu_batch **out);
-/* One persistent launch per value type (plus counter resets). */
+/* One persistent launch per group (plus counter resets); the groups'
+ * launches are forked onto the batch's own streams and joined back into
+ * `stream`, so they may run concurrently. */
 flsgpu_status flsgpu_batch_decompress(flsgpu_batch *batch, flsgpu_stream stream);
 /* Captures flsgpu_batch_decompress into a CUDA graph held by the batch
  * (NULL stream: a private stream is used); flsgpu_batch_replay launches it. */

@@ -8,7 +8,7 @@
 // space (prefix sums of the per-column vector counts), which a persistent
 // grid of warps consumes in chunks from an atomic counter (batch.cuh), so
 // short and long columns load-balance and a batch costs one launch per value
-// type present (at most four).  Per vector the warp dispatches on the
+// type and float kind present (at most six).  Per vector the warp dispatches on the
 // column's encoding and the vector's bit width to the same per-width
 // unpackers and autotuned policies as the single-column kernels.
 #include <cstdlib>
@@ -28,17 +28,23 @@ struct flsgpu_batch {
   std::vector<flsb200::BatchEntry> host_table;    // grouped by type
   std::vector<size_t> host_prefix;                // per group, n + 1 entries each
   std::vector<flsgpu_batch_column> cols;          // for the per-column path
-  int group_cols[4] = {0, 0, 0, 0};
-  size_t group_first[4] = {0, 0, 0, 0};           // first entry of each group
-  size_t group_prefix_at[4] = {0, 0, 0, 0};       // first prefix slot of each group
-  size_t group_vecs[4] = {0, 0, 0, 0};
+  // group g = 2 * value type + (ALP extended ? 1 : 0)
+  int group_cols[8] = {};
+  size_t group_first[8] = {};                     // first entry of each group
+  size_t group_prefix_at[8] = {};                 // first prefix slot of each group
+  size_t group_vecs[8] = {};
   flsb200::BatchEntry *d_table = nullptr;
   size_t *d_prefix = nullptr;
-  unsigned long long *d_counter = nullptr;        // one per group
+  unsigned long long *d_counter = nullptr;        // one per group (8)
   int n_cols = 0;
   size_t total_vecs = 0;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+  // fork / join of the per-type launches: they run concurrently, so one
+  // group's tail overlaps the next group's start
+  cudaStream_t side[7] = {};
+  cudaEvent_t ev_fork = nullptr;
+  cudaEvent_t ev_join[7] = {};
   flsgpu_decode_opts opts{};
   bool has_opts = false;
 };
@@ -84,14 +90,24 @@ static flsgpu_status fill_entry(BatchEntry &e, const flsgpu_batch_column &bc,
 
 static flsgpu_status launch_batch(flsgpu_batch *b, cudaStream_t s) {
   using L = flsgpu_status (*)(const BatchEntry *, const size_t *, int, size_t,
-                              unsigned long long *, cudaStream_t);
+                              unsigned long long *, cudaStream_t, int);
   static const L launch[4] = {launch_batch_u32, launch_batch_u64, launch_batch_f32,
                               launch_batch_f64};
-  for (int g = 0; g < 4; ++g) {
-    if (b->group_vecs[g] == 0) continue;
-    flsgpu_status st = launch[g](b->d_table + b->group_first[g], b->d_prefix + b->group_prefix_at[g],
-                                 b->group_cols[g], b->group_vecs[g], b->d_counter + g, s);
-    if (st) return st;
+  int groups[8], n = 0;
+  for (int g = 0; g < 8; ++g)
+    if (b->group_vecs[g] != 0) groups[n++] = g;
+  flsgpu_status st;
+  if (n > 1 && (st = check_cuda(cudaEventRecord(b->ev_fork, s), "fork"))) return st;
+  for (int i = 0; i < n; ++i) {
+    const int g = groups[i];
+    cudaStream_t gs = i == 0 ? s : b->side[i - 1];
+    if (i > 0 && (st = check_cuda(cudaStreamWaitEvent(gs, b->ev_fork, 0), "fork wait"))) return st;
+    if ((st = launch[g >> 1](b->d_table + b->group_first[g], b->d_prefix + b->group_prefix_at[g],
+                             b->group_cols[g], b->group_vecs[g], b->d_counter + g, gs, g & 1)))
+      return st;
+    if (i > 0 && ((st = check_cuda(cudaEventRecord(b->ev_join[i - 1], gs), "join")) ||
+                  (st = check_cuda(cudaStreamWaitEvent(s, b->ev_join[i - 1], 0), "join wait"))))
+      return st;
   }
   return FLSGPU_OK;
 }
@@ -128,12 +144,14 @@ flsgpu_status flsgpu_batch_create(const flsgpu_batch_column *columns, size_t n_c
     }
   }
   // group by type: table entries in group order, one prefix array per group
-  for (int g = 0; g < 4; ++g) {
+  for (int g = 0; g < 8; ++g) {
     b->group_first[g] = b->host_table.size();
     b->group_prefix_at[g] = b->host_prefix.size();
     b->host_prefix.push_back(0);
     for (size_t i = 0; i < n_columns; ++i) {
-      if ((int)columns[i].type != g) continue;
+      const int gi = 2 * (int)columns[i].type +
+                     (columns[i].encoding == FLSGPU_ENCODING_ALP_EXTENDED ? 1 : 0);
+      if (gi != g) continue;
       b->host_table.push_back(entries[i]);
       b->host_prefix.push_back(b->host_prefix.back() + entries[i].p.c.n_vecs);
       b->group_cols[g]++;
@@ -142,9 +160,18 @@ flsgpu_status flsgpu_batch_create(const flsgpu_batch_column *columns, size_t n_c
     b->total_vecs += b->group_vecs[g];
   }
   const size_t tb = sizeof(BatchEntry) * (b->host_table.size() ? b->host_table.size() : 1);
+  for (int i = 0; i < 7 && !s; ++i)
+    s = check_cuda(cudaStreamCreateWithFlags(&b->side[i], cudaStreamNonBlocking), "stream");
+  for (int i = 0; i < 7 && !s; ++i)
+    s = check_cuda(cudaEventCreateWithFlags(&b->ev_join[i], cudaEventDisableTiming), "event");
+  if (!s) s = check_cuda(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming), "event");
+  if (s) {
+    flsgpu_batch_destroy(b);
+    return s;
+  }
   if ((s = check_cuda(cudaMalloc(&b->d_table, tb), "cudaMalloc table")) ||
       (s = check_cuda(cudaMalloc(&b->d_prefix, sizeof(size_t) * b->host_prefix.size()), "cudaMalloc prefix")) ||
-      (s = check_cuda(cudaMalloc(&b->d_counter, 4 * sizeof(unsigned long long)), "cudaMalloc counter"))) {
+      (s = check_cuda(cudaMalloc(&b->d_counter, 8 * sizeof(unsigned long long)), "cudaMalloc counter"))) {
     flsgpu_batch_destroy(b);
     return s;
   }
@@ -252,6 +279,11 @@ void flsgpu_batch_destroy(flsgpu_batch *b) {
   if (b->d_table) cudaFree(b->d_table);
   if (b->d_prefix) cudaFree(b->d_prefix);
   if (b->d_counter) cudaFree(b->d_counter);
+  for (int i = 0; i < 7; ++i) {
+    if (b->side[i]) cudaStreamDestroy(b->side[i]);
+    if (b->ev_join[i]) cudaEventDestroy(b->ev_join[i]);
+  }
+  if (b->ev_fork) cudaEventDestroy(b->ev_fork);
   delete b;
 }
 

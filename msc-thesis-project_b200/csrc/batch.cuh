@@ -33,14 +33,23 @@ __device__ __forceinline__ int find_column(const size_t *prefix, int n_cols, siz
   return lo;
 }
 
-template <typename T> constexpr int batch_min_blocks() { return sizeof(T) == 4 ? 2 : 1; }
+// f64 ALP decodes faster register-capped at two blocks per SM (wide widths
+// in two runs of 16 values), as the single-column autotuning found; u64
+// FFOR keeps the register-rich kernel.
+template <typename T> constexpr int batch_var() {
+  return std::is_same<T, double>::value ? (VAR_DEFAULT | VAR_OCC) : VAR_DEFAULT;
+}
+template <typename T> constexpr int batch_min_blocks() { return min_blocks<T, batch_var<T>()>(); }
 
 // Persistent decode of every vector of a group of columns of one value
 // type.  Warps take chunks of kBatchChunk vectors of the group's index space
 // from an atomic counter; the column descriptor is staged in shared memory
 // when a warp moves to another column; the next vector's metadata is loaded
 // before the current one is decoded when both are in the same column.
-template <typename T>
+// XK: the group's float column kind (K_ALP or K_ALPX; one kernel each so
+// that neither carries the other's registers); integer groups mix BP and
+// FFOR columns (XK = K_FFOR).
+template <typename T, int XK>
 __global__ void __launch_bounds__(256, batch_min_blocks<T>())
     k_batch(const BatchEntry *__restrict__ table, const size_t *__restrict__ prefix, int n_cols,
             unsigned long long *counter) {
@@ -75,13 +84,11 @@ __global__ void __launch_bounds__(256, batch_min_blocks<T>())
       const uint32_t kind = s_kind[wib];
       const size_t vi = v - prefix[c];
       if constexpr (FLOAT) {
-        const Meta<T> cur = have_meta ? meta : load_meta<T, K_ALP>(p.c, vi);
+        (void)kind;
+        const Meta<T> cur = have_meta ? meta : load_meta<T, XK>(p.c, vi);
         have_meta = v + 1 < end && v + 1 < prefix[c + 1];
-        if (have_meta) meta = load_meta<T, K_ALP>(p.c, vi + 1);
-        if (kind == K_ALPX)
-          store_one<T, K_ALPX, VAR_DEFAULT>(p, vi, cur, t);
-        else
-          store_one<T, K_ALP, VAR_DEFAULT>(p, vi, cur, t);
+        if (have_meta) meta = load_meta<T, XK>(p.c, vi + 1);
+        store_one<T, XK, batch_var<T>()>(p, vi, cur, t);
       } else {
         const Meta<T> cur = have_meta ? meta
                             : (kind == K_BP ? load_meta<T, K_BP>(p.c, vi)
@@ -98,26 +105,37 @@ __global__ void __launch_bounds__(256, batch_min_blocks<T>())
   }
 }
 
-template <typename T> struct BatchLauncher {
+template <typename T, int XK> struct BatchLauncher {
   static int blocks_per_sm() {
     static int bps = 0;
     if (bps == 0) {
       int b = 0;
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_batch<T>, 256, 0);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_batch<T, XK>, 256, 0);
       bps = b > 0 ? b : 1;
     }
     return bps;
   }
+  static flsgpu_status launch(const BatchEntry *table, const size_t *prefix, int n_cols,
+                              size_t total_vecs, unsigned long long *counter, cudaStream_t s) {
+    flsgpu_status st =
+        check_cuda(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s), "memset");
+    if (st) return st;
+    const unsigned grid = persistent_blocks(total_vecs ? total_vecs : 1, 8, blocks_per_sm());
+    k_batch<T, XK><<<grid, 256, 0, s>>>(table, prefix, n_cols, counter);
+    note_launch();
+    return check_cuda(cudaGetLastError(), "k_batch launch");
+  }
 };
 
-// Launches k_batch<T> over one group (defined in batch_{u32,u64,f32,f64}.cu).
+// Launches k_batch over one group (defined in batch_{u32,u64,f32,f64}.cu);
+// alpx selects the ALP-extended kernel of the float types.
 flsgpu_status launch_batch_u32(const BatchEntry *, const size_t *, int, size_t,
-                               unsigned long long *, cudaStream_t);
+                               unsigned long long *, cudaStream_t, int alpx);
 flsgpu_status launch_batch_u64(const BatchEntry *, const size_t *, int, size_t,
-                               unsigned long long *, cudaStream_t);
+                               unsigned long long *, cudaStream_t, int alpx);
 flsgpu_status launch_batch_f32(const BatchEntry *, const size_t *, int, size_t,
-                               unsigned long long *, cudaStream_t);
+                               unsigned long long *, cudaStream_t, int alpx);
 flsgpu_status launch_batch_f64(const BatchEntry *, const size_t *, int, size_t,
-                               unsigned long long *, cudaStream_t);
+                               unsigned long long *, cudaStream_t, int alpx);
 
 }  // namespace flsb200

@@ -1,17 +1,13 @@
-// batch_f32.cu -- k_batch<float> (see batch.cuh).
+// batch_f32.cu -- the batched decode kernels of float columns (see batch.cuh).
 #include "batch.cuh"
 
 namespace flsb200 {
 
 flsgpu_status launch_batch_f32(const BatchEntry *table, const size_t *prefix, int n_cols,
-                               size_t total_vecs, unsigned long long *counter, cudaStream_t s) {
-  flsgpu_status st = check_cuda(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s), "memset");
-  if (st) return st;
-  const unsigned grid = persistent_blocks(total_vecs ? total_vecs : 1, 8,
-                                          BatchLauncher<float>::blocks_per_sm());
-  k_batch<float><<<grid, 256, 0, s>>>(table, prefix, n_cols, counter);
-  note_launch();
-  return check_cuda(cudaGetLastError(), "k_batch launch");
+                               size_t total_vecs, unsigned long long *counter, cudaStream_t s,
+                               int alpx) {
+  if (alpx) return BatchLauncher<float, K_ALPX>::launch(table, prefix, n_cols, total_vecs, counter, s);
+  return BatchLauncher<float, K_ALP>::launch(table, prefix, n_cols, total_vecs, counter, s);
 }
 
 }  // namespace flsb200

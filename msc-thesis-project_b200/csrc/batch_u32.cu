@@ -1,17 +1,13 @@
-// batch_u32.cu -- k_batch<uint32_t> (see batch.cuh).
+// batch_u32.cu -- the batched decode kernels of uint32_t columns (see batch.cuh).
 #include "batch.cuh"
 
 namespace flsb200 {
 
 flsgpu_status launch_batch_u32(const BatchEntry *table, const size_t *prefix, int n_cols,
-                               size_t total_vecs, unsigned long long *counter, cudaStream_t s) {
-  flsgpu_status st = check_cuda(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s), "memset");
-  if (st) return st;
-  const unsigned grid = persistent_blocks(total_vecs ? total_vecs : 1, 8,
-                                          BatchLauncher<uint32_t>::blocks_per_sm());
-  k_batch<uint32_t><<<grid, 256, 0, s>>>(table, prefix, n_cols, counter);
-  note_launch();
-  return check_cuda(cudaGetLastError(), "k_batch launch");
+                               size_t total_vecs, unsigned long long *counter, cudaStream_t s,
+                               int alpx) {
+  (void)alpx;
+  return BatchLauncher<uint32_t, K_FFOR>::launch(table, prefix, n_cols, total_vecs, counter, s);
 }
 
 }  // namespace flsb200
