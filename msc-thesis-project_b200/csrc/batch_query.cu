@@ -1,15 +1,17 @@
 // batch_query.cu -- fused per-pair query over compressed columns:
 //   result[i] = sum of A_i[k] over the positions k with B_i[k] < median(B_i)
 // for pairs (A_i: f64 ALP column, B_i: u32 FFOR column of the same length),
-// all pairs in one graph of six kernel kinds:
+// all pairs in one graph of four kernel kinds:
 //   * 4 radix-select passes over B (8 bits each, most significant first):
-//     each pass decodes B straight from its packed form and histograms the
-//     digit of the values that match the prefix chosen so far
-//     (k_pq_hist), then one warp per pair picks the digit that holds the
+//     each pass histograms the digit of the values that match the prefix
+//     chosen so far (k_pq_hist), using each vector's FFOR interval
+//     [base, base + 2^w - 1] to skip it or count it whole without decoding
+//     where it can, then one warp per pair picks the digit that holds the
 //     rank floor((n-1)/2) (k_pq_select);
-//   * one pass that decodes B and A of each vector into shared memory
-//     (A patched) and adds the A values whose B is below the median in the
-//     fixed order of the f64 sums (k_pq_sum), one partial per vector;
+//   * one pass that adds, per vector, the A values whose B is below the
+//     median in the fixed order of the f64 sums (k_pq_sum), one partial per
+//     vector, decoding B only for vectors whose interval holds the median
+//     and A only for vectors with a selected value;
 //   * one block per pair reduces its partials pairwise (k_pq_pairwise).
 // The reference has no such query; its multi-column kernel is the model for
 // decoding several columns of the same vector in lockstep
@@ -32,7 +34,7 @@ struct PairState {
   uint32_t rank;    // rank still to find among the values matching prefix
 };
 
-constexpr int kPairChunk = 16;
+constexpr int kPairChunk = 32;  // vectors per atomic: one per lane of the deciding warp
 
 __device__ __forceinline__ int find_pair(const size_t *prefix, int n, size_t v, int hint) {
   if (hint >= 0 && v >= prefix[hint] && v < prefix[hint + 1]) return hint;
@@ -55,8 +57,15 @@ __device__ __forceinline__ void flush_hist(uint32_t *sh, uint32_t *gh, int t) {
   }
 }
 
-// Radix-select histogram of pass `pass` (0..3) over every B vector.
-__global__ void __launch_bounds__(256)
+// Radix-select histogram of pass `pass` (0..3) over every B vector.  A
+// vector's values lie in [base, base + 2^w - 1] (when that does not wrap
+// past 2^32): if the interval misses the prefix chosen so far the vector is
+// skipped, and if it falls in one bin of this pass its valid values are
+// counted there without decoding; only the rest are decoded.  A warp takes
+// 32 vectors at a time and decides them in parallel, one per lane (one
+// round trip for all their metadata), then decodes the undecided ones
+// together.
+__global__ void __launch_bounds__(256, 2)
     k_pq_hist(const PairEntry *__restrict__ pairs, const size_t *__restrict__ prefix, int n_pairs,
               const PairState *__restrict__ state, uint32_t *hist, int pass,
               unsigned long long *counter, uint32_t *d_status) {
@@ -67,35 +76,71 @@ __global__ void __launch_bounds__(256)
   __syncwarp();
   const size_t total = prefix[n_pairs];
   const int shift = 24 - 8 * pass;
-  int cur = -1;
-  uint32_t want = 0;
+  int cur = -1;  // pair of the shared histogram
+  int hint = -1;
   while (true) {
     unsigned long long base = 0;
     if (t == 0) base = atomicAdd(counter, (unsigned long long)kPairChunk);
     base = __shfl_sync(0xffffffffu, base, 0);
     if (base >= total) break;
-    const size_t end = base + kPairChunk < total ? base + kPairChunk : total;
-    for (size_t v = base; v < end; ++v) {
-      const int pi = find_pair(prefix, n_pairs, v, cur);
-      if (pi != cur) {
+    // decide, one vector per lane
+    const size_t v = base + t;
+    int pi = -1, lim = 0, w = 0;
+    size_t off = 0;
+    uint32_t bbase = 0;
+    bool decode = false;
+    if (v < total) {
+      pi = find_pair(prefix, n_pairs, v, hint);
+      const ColumnParams &c = pairs[pi].b;
+      const size_t vi = v - prefix[pi];
+      const Meta<uint32_t> m = load_meta<uint32_t, K_FFOR>(c, vi);
+      const uint32_t *vin;
+      XInt<uint32_t> xf;
+      if (setup_from_meta<uint32_t, K_FFOR>(c, d_status, m, 0, vin, w, xf)) {
+        const size_t rem = c.n_values - vi * VEC;
+        lim = rem < (size_t)VEC ? (int)rem : VEC;
+        off = m.off;
+        bbase = m.base;
+        const uint32_t want = pass ? state[pi].prefix >> (shift + 8) : 0u;
+        const uint64_t lo = m.base, hi = lo + ((1ull << w) - 1ull);
+        decode = true;
+        if (hi <= 0xFFFFFFFFull) {
+          const uint64_t tlo = lo >> (shift + 8), thi = hi >> (shift + 8);
+          const uint32_t dlo = (uint32_t)(lo >> shift) & 255u, dhi = (uint32_t)(hi >> shift) & 255u;
+          if (pass > 0 && (thi < want || tlo > want)) {
+            decode = false;  // no value matches the prefix
+          } else if ((pass == 0 || (tlo == want && thi == want)) && dlo == dhi) {
+            decode = false;  // every valid value falls in one bin
+            atomicAdd(hist + 256 * (size_t)pi + dlo, (uint32_t)lim);
+          }
+        }
+      }
+    }
+    hint = __shfl_sync(0xffffffffu, pi, 31);
+    if (hint < 0) hint = __shfl_sync(0xffffffffu, pi, 0);
+    unsigned todo = __ballot_sync(0xffffffffu, decode);
+    while (todo) {
+      const int j = __ffs(todo) - 1;
+      todo &= todo - 1;
+      const int pj = __shfl_sync(0xffffffffu, pi, j);
+      const int wj = __shfl_sync(0xffffffffu, w, j);
+      const int limj = __shfl_sync(0xffffffffu, lim, j);
+      const uint32_t basej = __shfl_sync(0xffffffffu, bbase, j);
+      const size_t offj = ((size_t)__shfl_sync(0xffffffffu, (uint32_t)(off >> 32), j) << 32) |
+                          __shfl_sync(0xffffffffu, (uint32_t)off, j);
+      if (pj != cur) {
         if (cur >= 0) {
           __syncwarp();
           flush_hist(sh, hist + 256 * (size_t)cur, t);
           __syncwarp();
         }
-        cur = pi;
-        want = pass ? state[pi].prefix >> (shift + 8) : 0u;
+        cur = pj;
       }
-      const ColumnParams &c = pairs[pi].b;
-      const size_t vi = v - prefix[pi];
-      const uint32_t *vin;
-      int w;
-      XInt<uint32_t> xf;
-      if (!vector_setup<uint32_t, K_FFOR>(c, d_status, vi, t, vin, w, xf)) continue;
-      const size_t rem = c.n_values - vi * VEC;
-      const int lim = rem < (size_t)VEC ? (int)rem : VEC;
-      decode_values<uint32_t>(vin, w, t, xf, [&](int idx, uint32_t x, auto...) {
-        const bool match = (idx < lim) && (pass == 0 || (x >> (shift + 8)) == want);
+      const uint32_t want = pass ? state[pj].prefix >> (shift + 8) : 0u;
+      const uint32_t *vin = reinterpret_cast<const uint32_t *>(pairs[pj].b.packed) + offj;
+      const XInt<uint32_t> xf{basej};
+      decode_values<uint32_t>(vin, wj, t, xf, [&](int idx, uint32_t x, auto...) {
+        const bool match = (idx < limj) && (pass == 0 || (x >> (shift + 8)) == want);
         if (match) atomicAdd(&sh[(x >> shift) & 255u], 1u);
       });
     }
@@ -154,59 +199,121 @@ __global__ void k_pq_select(int n_pairs, PairState *state, uint32_t *hist, int p
   }
 }
 
-// Masked sum: per vector, decode B (u32) and A (f64, patched) into shared
-// memory, then thread t adds A[idx] for idx = t%16 + 16*(32*(t/16) + k),
-// k ascending, where B[idx] < median; warp butterfly -> partial.
-__global__ void __launch_bounds__(256)
+// Masked sum.  Per vector, thread t adds A[idx] for idx = t%16 +
+// 16*(32*(t/16) + k), k ascending, where B[idx] < median (the order of the
+// f64 sums); warp butterfly -> partial.
+// B's interval [base, base + 2^w - 1] decides without decoding B when it
+// lies wholly below the median (every valid value selected) or at or above
+// it (the vector adds nothing and A is not read); otherwise B is decoded
+// into one selection bit per value, and the bits a thread needs come from
+// the two B lanes that hold its positions (shuffles).  A is decoded into
+// the warp's shared memory and patched there before the sum.
+__global__ void __launch_bounds__(256, 2)
     k_pq_sum(const PairEntry *__restrict__ pairs, const size_t *__restrict__ prefix, int n_pairs,
              const PairState *__restrict__ state, double *partials, unsigned long long *counter,
              uint32_t *d_status) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int t = threadIdx.x & 31, wib = threadIdx.x >> 5;
   double *sa = reinterpret_cast<double *>(smem_raw) + wib * VEC;
-  uint32_t *sb = reinterpret_cast<uint32_t *>(smem_raw + 8 * VEC * sizeof(double)) + wib * VEC;
   const size_t total = prefix[n_pairs];
-  int cur = -1;
+  const int lane = t & 15, half = t >> 4;
+  int hint = -1;
   while (true) {
     unsigned long long base = 0;
     if (t == 0) base = atomicAdd(counter, (unsigned long long)kPairChunk);
     base = __shfl_sync(0xffffffffu, base, 0);
     if (base >= total) break;
-    const size_t end = base + kPairChunk < total ? base + kPairChunk : total;
-    for (size_t v = base; v < end; ++v) {
-      const int pi = find_pair(prefix, n_pairs, v, cur);
-      cur = pi;
-      const uint32_t med = state[pi].prefix;
-      const size_t vi = v - prefix[pi];
+    // decide, one vector per lane: 0 nothing selected, 1 all, 2 decode B
+    const size_t v = base + t;
+    int pi = -1, mode = 0;
+    if (v < total) {
+      pi = find_pair(prefix, n_pairs, v, hint);
       const PairEntry &pe = pairs[pi];
+      const size_t vi = v - prefix[pi];
+      const Meta<uint32_t> mb = load_meta<uint32_t, K_FFOR>(pe.b, vi);
+      const uint32_t med = state[pi].prefix;
+      const uint64_t lo = mb.base, hi = lo + ((1ull << (mb.w <= 32 ? mb.w : 0)) - 1ull);
+      mode = 2;
+      if (mb.w <= 32 && hi <= 0xFFFFFFFFull) mode = hi < med ? 1 : lo >= med ? 0 : 2;
+      if (mode == 0) partials[v] = 0.0;
+      else if (mode == 2 && mb.w <= 32) {
+        // this lane's straddling vector: its B lines into L2 now
+        const char *pb = reinterpret_cast<const char *>(
+            reinterpret_cast<const uint32_t *>(pe.b.packed) + mb.off);
+        for (int l = 0; l < mb.w; ++l) asm volatile("prefetch.global.L2 [%0];" ::"l"(pb + 128 * l));
+      }
+    }
+    hint = __shfl_sync(0xffffffffu, pi, 31);
+    if (hint < 0) hint = __shfl_sync(0xffffffffu, pi, 0);
+    unsigned todo = __ballot_sync(0xffffffffu, mode != 0);
+    while (todo) {
+      const int j = __ffs(todo) - 1;
+      todo &= todo - 1;
+      const int pj = __shfl_sync(0xffffffffu, pi, j);
+      const bool all = __shfl_sync(0xffffffffu, mode, j) == 1;
+      const size_t vj = base + j;
+      const uint32_t med = state[pj].prefix;
+      const size_t vi = vj - prefix[pj];
+      const PairEntry &pe = pairs[pj];
+      const Meta<double> ma = load_meta<double, K_ALP>(pe.a, vi);
+      const Meta<uint32_t> mb = load_meta<uint32_t, K_FFOR>(pe.b, vi);
       double acc = 0.0;
       const uint32_t *bin;
       const uint64_t *ain;
       int wb, wa;
       XInt<uint32_t> xb;
       XAlpF64 xa;
-      const bool okb = vector_setup<uint32_t, K_FFOR>(pe.b, d_status, vi, t, bin, wb, xb);
-      const bool oka = vector_setup<double, K_ALP>(pe.a, d_status, vi, t, ain, wa, xa);
+      const bool okb = setup_from_meta<uint32_t, K_FFOR>(pe.b, d_status, mb, t, bin, wb, xb);
+      const bool oka = setup_from_meta<double, K_ALP>(pe.a, d_status, ma, t, ain, wa, xa);
       const size_t rem = pe.a.n_values - vi * VEC;
       const int lim = rem < (size_t)VEC ? (int)rem : VEC;
       if (okb && oka) {
-        decode_values<uint32_t>(bin, wb, t, xb, [&](int idx, uint32_t x, auto...) { sb[idx] = x; });
-        decode_values<double>(ain, wa, t, xa, [&](int idx, double x, auto...) { sa[idx] = x; });
+        const uint32_t ecnt = pe.a.patch ? ma.ecnt : 0u;
+        const double *exc = reinterpret_cast<const double *>(pe.a.exc);
+        uint32_t p0 = VEC;
+        double e0 = 0.0;
+        if ((uint32_t)t < ecnt) {
+          p0 = pe.a.pos[ma.eo + t];
+          e0 = exc[ma.eo + t];
+        }
+        uint32_t selA = 0, selB = 0;
+        if (!all) {
+          prefetch_packed(ain, wa, t);  // A's lines come into L2 while B decodes
+          uint32_t bits = 0;
+          decode_values<uint32_t>(bin, wb, t, xb, [&](int idx, uint32_t x, auto...) {
+            if (idx < lim && x < med) bits |= 1u << (idx >> 5);
+          });
+          selA = __shfl_sync(0xffffffffu, bits, lane);
+          selB = __shfl_sync(0xffffffffu, bits, lane + 16);
+        }
+        // A into shared memory (a plain store per value keeps this decode's
+        // code as small as the single-column kernels'), patched, then summed
+        decode_values<double, VAR_DEFAULT | VAR_OCC>(ain, wa, t, xa,
+                                                    [&](int idx, double x, auto...) { sa[idx] = x; });
         __syncwarp();
-        if (pe.a.patch)
-          patch_vector<double, K_ALP>(pe.a, d_status, vi, t, [&](int ps, double e) { sa[ps] = e; });
+        bool bad = (uint32_t)t < ecnt && p0 >= VEC;
+        if (p0 < VEC) sa[p0] = e0;
+        for (uint32_t i = t + 32; i < ecnt; i += 32) {
+          const uint32_t ps = pe.a.pos[ma.eo + i];
+          if (ps < VEC)
+            sa[ps] = exc[ma.eo + i];
+          else
+            bad = true;
+        }
+        if (__any_sync(0xffffffffu, bad) && t == 0) flag_status(d_status, FLSGPU_BAD_EXCEPTION);
         __syncwarp();
-        const int lane = t & 15, half = t >> 4;
 #pragma unroll 8
         for (int k = 0; k < 32; ++k) {
           const int idx = lane + 16 * (32 * half + k);
-          if (idx < lim && sb[idx] < med) acc = __dadd_rn(acc, sa[idx]);
+          const bool sel = all ? idx < lim
+                               : ((((k & 1) ? selB : selA) >> (16 * half + (k >> 1))) & 1u) != 0;
+          if (sel) acc = __dadd_rn(acc, sa[idx]);
         }
         __syncwarp();
       }
 #pragma unroll
       for (int s = 16; s >= 1; s >>= 1) acc = __dadd_rn(acc, __shfl_xor_sync(0xffffffffu, acc, s));
-      if (t == 0) partials[v] = acc;
+      if (t == 0) partials[vj] = acc;
     }
   }
 }
@@ -266,7 +373,7 @@ struct flsgpu_pair_query {
 
 namespace flsb200 {
 
-constexpr size_t kPqSumSmem = 8 * VEC * (sizeof(double) + sizeof(uint32_t));
+constexpr size_t kPqSumSmem = 8 * VEC * sizeof(double);
 constexpr int kMaxPairVectors = 2048 * 1024;  // chunk results per block (k_pq_pairwise)
 
 static flsgpu_status pq_launch(flsgpu_pair_query *q, cudaStream_t s) {
