@@ -132,9 +132,17 @@ flsgpu_status flsgpu_alp_encode_f64(flsgpu_alp_encoder *encoder, const double *d
                                     size_t n_values, uint32_t mode,
                                     flsgpu_alp_encode_result *out, flsgpu_stream stream);
 /* pieces exposed for tests and tools */
+/* Top-k (k <= 4) proposed classes per vector in one fused kernel (features,
+ * the three layers on the tensor cores with activations kept in shared
+ * memory, top-k); _layered runs the same arithmetic as separate launches
+ * (features, three GEMMs, top-k) and gives the same classes. */
 flsgpu_status flsgpu_alp_encoder_propose(flsgpu_alp_encoder *encoder, const double *d_values,
                                          size_t n_values, uint32_t k, int16_t *d_cand,
                                          flsgpu_stream stream);
+flsgpu_status flsgpu_alp_encoder_propose_layered(flsgpu_alp_encoder *encoder,
+                                                 const double *d_values, size_t n_values,
+                                                 uint32_t k, int16_t *d_cand,
+                                                 flsgpu_stream stream);
 flsgpu_status flsgpu_alp_plain_labels(const double *d_values, size_t n_values, int16_t *d_labels,
                                       int32_t *d_estimates, flsgpu_stream stream);
 flsgpu_status flsgpu_alp_features(const double *d_values, size_t n_values, void *d_features_bf16,

@@ -87,22 +87,96 @@ __device__ __forceinline__ int sample_estimate(double s, int e, int f, bool skip
   return 32 * bits + (32 - nonexc) * (64 + 16);
 }
 
-// Exhaustive search over the 190 pairs (0 <= f <= e <= 18), tie rules of
-// find_top_k_combinations; returns the class (pair index e*(e+1)/2 + f, or
-// kClassRD when the best estimate reaches the ALP-RD limit 48*32).
-__device__ int plain_search(double s, int *est_out, int *pair_out = nullptr) {
-  int sbest = 32 * (64 + 16) + 32 * 64;
-  int fe = 0, ff = 0;
-  for (int e = 18; e >= 0; --e) {
-    for (int f = e; f >= 0; --f) {
-      const int est = sample_estimate(s, e, f, true);
-      if (est < 0) continue;
-      if (est < sbest || (est == sbest && fe < e) || (est == sbest && fe == e && ff < f)) {
-        sbest = est;
-        fe = e;
-        ff = f;
+// Exhaustive search over the 190 pairs (0 <= f <= e <= 18) on the warp's
+// 32 samples (smp, shared memory), with the estimate and tie rules of
+// find_top_k_combinations.  Lane l evaluates the pairs of class l, l + 32,
+// ... over all samples, so no per-pair warp reduction is needed; a single
+// warp minimum over (estimate, 18 - e, 18 - f) then picks the pair the
+// reference's sequential scan keeps (e from 18 down, f from e down,
+// replacing only on a strictly lower estimate: among equal estimates the
+// first one scanned, i.e. the highest e, then the highest f).  Returns the
+// class (e * (e + 1) / 2 + f), or kClassRD when the best estimate reaches
+// the ALP-RD limit 48 * 32; without any pair that round-trips at least two
+// samples the result is pair (0, 0) at the initial estimate, as the scan's.
+__device__ int plain_search(const double *smp, int t, int *est_out, int *pair_out = nullptr) {
+  constexpr int P = 3;  // pairs per round; two rounds cover ceil(190 / 32) = 6
+  uint32_t key = 0xFFFFFFFFu;
+#pragma unroll 1
+  for (int round = 0; round < 2; ++round) {
+    // per pair: 10^e, 10^-f, 10^f (as a double) and 10^-e in registers
+    // (lanes index the constant tables differently, so they are read once)
+    double m10e[P], mfrf[P], factd[P], frce[P], dmn[P], dmx[P];
+    int64_t mn[P], mx[P];
+    int cnt[P], pe[P], pf[P];
+#pragma unroll
+    for (int i = 0; i < P; ++i) {
+      const int c = t + 32 * (round * P + i);
+      const int e = c < kClassRD ? class_exp(c) : 0, f = c < kClassRD ? c - e * (e + 1) / 2 : 0;
+      pe[i] = e;
+      pf[i] = f;
+      m10e[i] = c_f64_exp10[e];
+      mfrf[i] = c_f64_frac[f];
+      factd[i] = (double)c_f64_fact[f];
+      frce[i] = c_f64_frac[e];
+      dmn[i] = 1e300;
+      dmx[i] = -1e300;
+      mn[i] = INT64_MAX;
+      mx[i] = INT64_MIN;
+      cnt[i] = 0;
+    }
+#pragma unroll 2
+    for (int k = 0; k < 32; ++k) {
+      const double x = smp[k];
+#pragma unroll
+      for (int i = 0; i < P; ++i) {
+        const double tv = __dmul_rn(__dmul_rn(x, m10e[i]), mfrf[i]);
+        const double r = __dsub_rn(__dadd_rn(tv, kMagic), kMagic);
+        const double p = __dmul_rn(r, factd[i]);
+        // |tv| < 2^51: r is the integer the reference's cast yields; |p| <
+        // 2^53: the reference's integer product, converted, is p exactly;
+        // -0.0 is the reference's "impossible" case
+        if (fabs(tv) < 2251799813685248.0 && fabs(p) < 9007199254740992.0 &&
+            __double_as_longlong(tv) != (long long)0x8000000000000000ull) {
+          if (__dmul_rn(p, frce[i]) == x) {
+            ++cnt[i];
+            dmn[i] = fmin(dmn[i], r);
+            dmx[i] = fmax(dmx[i], r);
+          }
+        } else {
+          const int64_t q = impossible_f64(tv) ? (int64_t)kEncUpper : cvtt_s64(r);
+          const double d = __dmul_rn(
+              __ll2double_rn((long long)((uint64_t)q * (uint64_t)c_f64_fact[pf[i]])), frce[i]);
+          if (d == x) {
+            ++cnt[i];
+            mn[i] = q < mn[i] ? q : mn[i];
+            mx[i] = q > mx[i] ? q : mx[i];
+          }
+        }
       }
     }
+#pragma unroll
+    for (int i = 0; i < P; ++i) {
+      const int c = t + 32 * (round * P + i);
+      if (c < kClassRD && cnt[i] >= 2) {
+        int64_t lo = mn[i], hi = mx[i];
+        if (dmn[i] <= dmx[i]) {
+          const int64_t a = (int64_t)dmn[i], b = (int64_t)dmx[i];
+          lo = a < lo ? a : lo;
+          hi = b > hi ? b : hi;
+        }
+        const int est = 32 * count_bits64((uint64_t)hi - (uint64_t)lo) + (32 - cnt[i]) * 80;
+        const uint32_t kk =
+            ((uint32_t)est << 10) | ((uint32_t)(18 - pe[i]) << 5) | (uint32_t)(18 - pf[i]);
+        key = kk < key ? kk : key;
+      }
+    }
+  }
+  key = __reduce_min_sync(0xffffffffu, key);
+  int sbest = 32 * (64 + 16) + 32 * 64, fe = 0, ff = 0;
+  if (key != 0xFFFFFFFFu) {
+    sbest = (int)(key >> 10);
+    fe = 18 - (int)((key >> 5) & 31);
+    ff = 18 - (int)(key & 31);
   }
   if (est_out) *est_out = sbest;
   if (pair_out) *pair_out = pair_class(fe, ff);
@@ -115,10 +189,14 @@ __global__ void __launch_bounds__(256) k_plain_labels(const double *__restrict__
                                                       int32_t *est) {
   const int t = threadIdx.x & 31;
   const size_t nw = ((size_t)gridDim.x * blockDim.x) >> 5;
+  __shared__ double s_smp[8][32];
+  double *smp = s_smp[threadIdx.x >> 5];
   for (size_t v = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n_vecs; v += nw) {
-    const double s = vals[v * VEC + 32 * t];
+    __syncwarp();
+    smp[t] = vals[v * VEC + 32 * t];
+    __syncwarp();
     int e;
-    const int cls = plain_search(s, &e);
+    const int cls = plain_search(smp, t, &e);
     if (t == 0) {
       labels[v] = (int16_t)cls;
       if (est) est[v] = e;
@@ -128,29 +206,45 @@ __global__ void __launch_bounds__(256) k_plain_labels(const double *__restrict__
 
 // ---- vector encode ---------------------------------------------------------
 // Thread t owns lane t % 16, values 32*(t/16) .. +31 of the lane (position
-// lane + 16*(32*half + k)).  Returns the exception count; fills the packed
-// FastLanes words (bw * 16 u64 at `packed`), the exceptions (value,
-// position) in ascending position order at `exc`/`pos`, base and width.
-__device__ int encode_vector(const double *__restrict__ vec, int e, int f, int t,
-                             uint64_t *packed, double *exc, uint16_t *pos, uint64_t *base_out,
-                             int *bw_out) {
+// lane + 16*(32*half + k)).  The encode runs in two kernels: the first
+// analyses each vector under its chosen (e, f) (exceptions, the fill
+// integer, base and width), the second, after the scan of the sizes,
+// recomputes the integers and writes the packed words and exceptions
+// straight to their final offsets.
+
+// encode_simdized's exception test for one value: specials (inf, NaN,
+// -0.0) are encoded as the upper bound and become exceptions.
+__device__ __forceinline__ int64_t enc_checked(double x, int f, int e, bool *is_exc) {
+  const uint64_t bits = (uint64_t)__double_as_longlong(x);
+  const bool special = ((bits & 0x7FFFFFFFFFFFFFFFull) >= 0x7FF0000000000000ull) ||
+                       bits == 0x8000000000000000ull;
+  const double a = special ? kEncUpper : x;
+  const int64_t q = enc_value(a, f, e, false);
+  *is_exc = dec_value(q, f, e) != a;
+  return q;
+}
+
+struct VecAnalysis {
+  int n_exc;
+  int bw;
+  int64_t fill;   // the integer stored at exception positions
+  uint64_t base;  // minimum of the stored integers
+};
+
+__device__ VecAnalysis analyze_vector(const double *__restrict__ vec, int e, int f, int t) {
   const int lane = t & 15, half = t >> 4;
-  // pass 1: exceptions, first non-exception position, min / max of the
-  // integers of the non-exceptions (the integers are recomputed in pass 2
-  // rather than held: 32 int64 per thread would cap occupancy)
   uint32_t exc_mask = 0;
   int first_ok = 1 << 30;
   int64_t mn = INT64_MAX, mx = INT64_MIN;
-#pragma unroll 4
+  // all 32 loads in flight before any use (the kernel is latency-bound)
+  double xv[32];
+#pragma unroll
+  for (int k = 0; k < 32; ++k) xv[k] = vec[lane + 16 * (32 * half + k)];
+#pragma unroll
   for (int k = 0; k < 32; ++k) {
     const int p = lane + 16 * (32 * half + k);
-    const double x = vec[p];
-    const uint64_t bits = (uint64_t)__double_as_longlong(x);
-    const bool special = ((bits & 0x7FFFFFFFFFFFFFFFull) >= 0x7FF0000000000000ull) ||
-                         bits == 0x8000000000000000ull;
-    const double a = special ? kEncUpper : x;
-    const int64_t q = enc_value(a, f, e, false);
-    const bool is_exc = dec_value(q, f, e) != a;
+    bool is_exc;
+    const int64_t q = enc_checked(xv[k], f, e, &is_exc);
     exc_mask |= (uint32_t)is_exc << k;
     if (!is_exc) {
       first_ok = min(first_ok, p);
@@ -160,36 +254,44 @@ __device__ int encode_vector(const double *__restrict__ vec, int e, int f, int t
   }
 #pragma unroll
   for (int s = 16; s >= 1; s >>= 1) first_ok = min(first_ok, __shfl_xor_sync(0xffffffffu, first_ok, s));
-  const int n_exc = __reduce_add_sync(0xffffffffu, __popc(exc_mask));
-  // the integer stored at exception positions: that of the first
-  // non-exception (0 when every position, or every position but the last,
-  // is an exception)
-  int64_t fill = 0;
-  if (first_ok < VEC && !(first_ok == VEC - 1 && n_exc == VEC - 1))
-    fill = enc_value(vec[first_ok], f, e, false);
+  VecAnalysis a;
+  a.n_exc = __reduce_add_sync(0xffffffffu, __popc(exc_mask));
+  // the first non-exception's integer (0 when every position, or every
+  // position but the last, is an exception: encoder.hpp:361-367)
+  a.fill = 0;
+  if (first_ok < VEC && !(first_ok == VEC - 1 && a.n_exc == VEC - 1))
+    a.fill = enc_value(vec[first_ok], f, e, false);
   if (exc_mask) {
-    mn = fill < mn ? fill : mn;
-    mx = fill > mx ? fill : mx;
+    mn = a.fill < mn ? a.fill : mn;
+    mx = a.fill > mx ? a.fill : mx;
   }
   mn = warp_min_s64(mn);
   mx = warp_max_s64(mx);
-  const int bw = count_bits64((uint64_t)mx - (uint64_t)mn);
-  const uint64_t base = (uint64_t)mn;
-  // pass 2, pack: this thread's 32 values are bits [32*half*bw,
-  // 32*(half+1)*bw) of the lane stream = its bw 32-bit words, owned by it
-  // alone
-  if (bw > 0) {
-    uint32_t *p32 = reinterpret_cast<uint32_t *>(packed) + 2 * lane;
-    const uint64_t mask = bw >= 64 ? ~0ull : ((1ull << bw) - 1);
-    uint32_t acc = 0;  // pending low bits (< 32 of them)
-    int nacc = 0, m = half * bw;
-#pragma unroll 4
-    for (int k = 0; k < 32; ++k) {
-      int64_t q = fill;
-      if (!((exc_mask >> k) & 1)) {
-        const double x = vec[lane + 16 * (32 * half + k)];
-        q = enc_value(x, f, e, false);
-      }
+  a.bw = count_bits64((uint64_t)mx - (uint64_t)mn);
+  a.base = (uint64_t)mn;
+  return a;
+}
+
+// Packed words (bw * 16 u64 at `packed`) and exceptions (value, position,
+// ascending position) at `exc` / `pos` of one vector, staged in the warp's
+// shared copy `sv` of the vector (filled and synchronised by the caller).
+__device__ void pack_vector(const double *sv, int e, int f, int t, int64_t fill, uint64_t base,
+                            int bw, uint64_t *packed, double *exc, uint16_t *pos) {
+  const int lane = t & 15, half = t >> 4;
+  uint32_t exc_mask = 0;
+  // this thread's 32 values are bits [32*half*bw, 32*(half+1)*bw) of the
+  // lane stream = its bw 32-bit words, owned by it alone
+  uint32_t *p32 = reinterpret_cast<uint32_t *>(packed) + 2 * lane;
+  const uint64_t mask = bw >= 64 ? ~0ull : ((1ull << bw) - 1);
+  uint32_t acc = 0;  // pending low bits (< 32 of them)
+  int nacc = 0, m = half * bw;
+#pragma unroll 2
+  for (int k = 0; k < 32; ++k) {
+    bool is_exc;
+    int64_t q = enc_checked(sv[lane + 16 * (32 * half + k)], f, e, &is_exc);
+    exc_mask |= (uint32_t)is_exc << k;
+    if (is_exc) q = fill;
+    if (bw > 0) {
       const uint64_t d = ((uint64_t)q - base) & mask;
       // (hi:lo) = acc | d << nacc, total = nacc + bw bits (at most 95)
       uint64_t lo = (uint64_t)acc | (d << nacc);
@@ -209,47 +311,49 @@ __device__ int encode_vector(const double *__restrict__ vec, int e, int f, int t
   // exceptions in ascending position: positions of round r = 16 * r + lane,
   // rounds 0..31 come from half 0, rounds 32..63 from half 1; only rounds
   // holding an exception are visited
+  const uint32_t any0 = __reduce_or_sync(0xffffffffu, half == 0 ? exc_mask : 0u);
+  const uint32_t any1 = __reduce_or_sync(0xffffffffu, half == 1 ? exc_mask : 0u);
+  uint64_t rounds = (uint64_t)any0 | ((uint64_t)any1 << 32);
   int written = 0;
-  if (n_exc) {
-    const uint32_t any0 = __reduce_or_sync(0xffffffffu, half == 0 ? exc_mask : 0u);
-    const uint32_t any1 = __reduce_or_sync(0xffffffffu, half == 1 ? exc_mask : 0u);
-    uint64_t rounds = (uint64_t)any0 | ((uint64_t)any1 << 32);
-    while (rounds) {
-      const int r = __ffsll((long long)rounds) - 1;
-      rounds &= rounds - 1;
-      const int h = r >> 5, k = r & 31;
-      const bool mine = (half == h) && ((exc_mask >> k) & 1);
-      const unsigned bal = __ballot_sync(0xffffffffu, mine);
-      if (mine) {
-        const int slot = written + __popc(bal & ((1u << t) - 1));
-        const int p = lane + 16 * r;
-        exc[slot] = vec[p];
-        pos[slot] = (uint16_t)p;
-      }
-      written += __popc(bal);
+  while (rounds) {
+    const int r = __ffsll((long long)rounds) - 1;
+    rounds &= rounds - 1;
+    const int h = r >> 5, k = r & 31;
+    const bool mine = (half == h) && ((exc_mask >> k) & 1);
+    const unsigned bal = __ballot_sync(0xffffffffu, mine);
+    if (mine) {
+      const int slot = written + __popc(bal & ((1u << t) - 1));
+      const int p = lane + 16 * r;
+      exc[slot] = sv[p];
+      pos[slot] = (uint16_t)p;
     }
+    written += __popc(bal);
   }
-  if (base_out) *base_out = base;
-  if (bw_out) *bw_out = bw;
-  return n_exc;
 }
 
-// One warp per vector.  mode 0: parameters from the plain search; mode 1:
-// candidates (k per vector, network order) verified on the samples with the
-// reference's second-level choice, plain search when the network proposes
-// ALP-RD or the encode leaves more than `max_exc` exceptions.
+// Parameters of every vector, one warp per vector.  mode 0: the plain
+// search; mode 1: candidates (k per vector, network order) chosen among on
+// the samples with the reference's second-level rule (encoder.hpp:237-300),
+// and the plain search when no candidate is an ALP pair or the choice leaves
+// more than `max_exc` exceptions in the vector.  Writes the vector's
+// exponent, factor, width, base, exception count, fill integer and flags
+// (bit 0: the plain search ran as fallback; bit 1: ALP-RD territory).
 __global__ void __launch_bounds__(256)
-    k_alp_encode(const double *__restrict__ vals, size_t n_vecs, int mode,
+    k_alp_choose(const double *__restrict__ vals, size_t n_vecs, int mode,
                  const int16_t *__restrict__ cand, int k_cand, int max_exc, EncodeSlots sl) {
+  __shared__ double s_smp[8][32];
+  double *smp = s_smp[threadIdx.x >> 5];
   const int t = threadIdx.x & 31;
   const size_t nw = ((size_t)gridDim.x * blockDim.x) >> 5;
   for (size_t v = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n_vecs; v += nw) {
     const double *vec = vals + v * VEC;
     const double s = vec[32 * t];
+    __syncwarp();
+    smp[t] = s;
+    __syncwarp();
     int cls = -1;
     bool fallback = false, rd_net = false;
     if (mode == 1) {
-      // second-level choice among the proposed pairs (encoder.hpp:237-300)
       int best = 0, worse = 0, chosen = -1;
       for (int c = 0; c < k_cand; ++c) {
         const int pc = cand[v * k_cand + c];
@@ -277,99 +381,202 @@ __global__ void __launch_bounds__(256)
     // ALPColumn, and the RD decision is reported through the flags.
     int pair = 0;
     if (mode == 0 || fallback) {
-      cls = plain_search(s, nullptr, &pair);
+      cls = plain_search(smp, t, nullptr, &pair);
     } else {
       pair = cls;
     }
     const bool rd = cls == kClassRD || rd_net;
     int e = class_exp(pair), f = class_fac(pair);
-    uint64_t base;
-    int bw;
-    int n_exc = encode_vector(vec, e, f, t, sl.packed + v * VEC, sl.exc + v * VEC,
-                              sl.pos + v * VEC, &base, &bw);
+    VecAnalysis a = analyze_vector(vec, e, f, t);
     // Fall back when the proposal leaves more than max_exc exceptions, ALP-RD
     // proposals included: their ALP pair is then the plain search's, so the
     // column's size never depends on how far the network's ALP candidates
     // are from the search's choice on high-exception vectors.
-    if (mode == 1 && !fallback && n_exc > max_exc) {
-      // the proposal leaves too many exceptions: plain search and re-encode
-      __syncwarp();
-      fallback = true;
-      int pc;
-      plain_search(s, nullptr, &pc);
-      e = class_exp(pc);
-      f = class_fac(pc);
-      n_exc = encode_vector(vec, e, f, t, sl.packed + v * VEC, sl.exc + v * VEC, sl.pos + v * VEC,
-                            &base, &bw);
+    // The search itself runs in k_alp_fallback over the listed vectors, so
+    // that the warps of this kernel all carry the same load.
+    if (mode == 1 && !fallback && a.n_exc > max_exc) {
+      if (t == 0) {
+        sl.fb_list[atomicAdd(sl.fb_count, 1u)] = (uint32_t)v;
+        sl.flags[v] = (uint8_t)(1 | (rd ? 2 : 0));
+      }
+      continue;
     }
     if (t == 0) {
-      sl.bw[v] = (uint8_t)bw;
-      sl.base[v] = base;
+      sl.bw[v] = (uint8_t)a.bw;
+      sl.base[v] = a.base;
+      sl.fill[v] = a.fill;
       sl.fac[v] = (uint8_t)f;
       sl.exp[v] = (uint8_t)e;
-      sl.count[v] = (uint16_t)n_exc;
+      sl.count[v] = (uint16_t)a.n_exc;
       sl.flags[v] = (uint8_t)((fallback ? 1 : 0) | (rd ? 2 : 0));
     }
   }
 }
 
-// Exclusive scan of per-vector sizes (packed words = bw * 16, exceptions)
-// in one block; n_vecs up to a few million.
-__global__ void __launch_bounds__(1024) k_scan_sizes(const uint8_t *bw, const uint16_t *count,
-                                                     size_t n, size_t *off_words,
-                                                     size_t *off_exc, size_t *totals) {
-  __shared__ size_t s_w[1024], s_e[1024];
-  const int tid = threadIdx.x;
-  const size_t per = (n + 1023) / 1024;
-  const size_t lo = tid * per, hi = min(n, lo + per);
-  size_t sw = 0, se = 0;
-  for (size_t i = lo; i < hi; ++i) {
-    sw += (size_t)bw[i] * 16;
-    se += count[i];
-  }
-  s_w[tid] = sw;
-  s_e[tid] = se;
-  __syncthreads();
-  for (int o = 1; o < 1024; o <<= 1) {
-    size_t aw = 0, ae = 0;
-    if (tid >= o) {
-      aw = s_w[tid - o];
-      ae = s_e[tid - o];
+// The plain search and analysis of the vectors k_alp_choose listed (their
+// proposal left more than max_exc exceptions); one warp per listed vector.
+__global__ void __launch_bounds__(256)
+    k_alp_fallback(const double *__restrict__ vals, EncodeSlots sl) {
+  __shared__ double s_smp[8][32];
+  double *smp = s_smp[threadIdx.x >> 5];
+  const int t = threadIdx.x & 31;
+  const size_t nw = ((size_t)gridDim.x * blockDim.x) >> 5;
+  const size_t n = *sl.fb_count;
+  for (size_t i = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nw) {
+    const size_t v = sl.fb_list[i];
+    const double *vec = vals + v * VEC;
+    __syncwarp();
+    smp[t] = vec[32 * t];
+    __syncwarp();
+    int pair;
+    plain_search(smp, t, nullptr, &pair);
+    const int e = class_exp(pair), f = class_fac(pair);
+    const VecAnalysis a = analyze_vector(vec, e, f, t);
+    if (t == 0) {
+      sl.bw[v] = (uint8_t)a.bw;
+      sl.base[v] = a.base;
+      sl.fill[v] = a.fill;
+      sl.fac[v] = (uint8_t)f;
+      sl.exp[v] = (uint8_t)e;
+      sl.count[v] = (uint16_t)a.n_exc;
     }
-    __syncthreads();
-    s_w[tid] += aw;
-    s_e[tid] += ae;
-    __syncthreads();
-  }
-  size_t rw = s_w[tid] - sw, re = s_e[tid] - se;
-  for (size_t i = lo; i < hi; ++i) {
-    off_words[i] = rw;
-    off_exc[i] = re;
-    rw += (size_t)bw[i] * 16;
-    re += count[i];
-  }
-  if (tid == 1023) {
-    totals[0] = s_w[1023];
-    totals[1] = s_e[1023];
   }
 }
 
-// Compaction into the contiguous column arrays: one warp per vector.
-__global__ void __launch_bounds__(256) k_compact(EncodeSlots sl, size_t n_vecs,
-                                                 const size_t *off_words, const size_t *off_exc,
-                                                 uint64_t *packed, double *exc, uint16_t *pos) {
+// Column statistics for the caller: totals[2] += fallbacks, totals[3] +=
+// ALP-RD vectors, totals[4] += the sum of the bit widths.
+__global__ void __launch_bounds__(256) k_encode_stats(const uint8_t *flags, const uint8_t *bw,
+                                                      size_t n, size_t *totals) {
+  size_t fb = 0, rd = 0, sbw = 0;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    fb += flags[i] & 1;
+    rd += (flags[i] >> 1) & 1;
+    sbw += bw[i];
+  }
+#pragma unroll
+  for (int s = 16; s >= 1; s >>= 1) {
+    fb += __shfl_xor_sync(0xffffffffu, fb, s);
+    rd += __shfl_xor_sync(0xffffffffu, rd, s);
+    sbw += __shfl_xor_sync(0xffffffffu, sbw, s);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd((unsigned long long *)&totals[2], (unsigned long long)fb);
+    atomicAdd((unsigned long long *)&totals[3], (unsigned long long)rd);
+    atomicAdd((unsigned long long *)&totals[4], (unsigned long long)sbw);
+  }
+}
+
+// Exclusive scan of the per-vector sizes (packed words = bw * 16,
+// exceptions) in three steps: per block of 1024 vectors (k_scan_local:
+// offsets within the block, block totals), over the block totals
+// (k_scan_blocks: one block; also the column totals), and the block offset
+// added by k_alp_pack, which writes the final offsets.
+__device__ __forceinline__ void block_excl_scan2(size_t &a, size_t &b, size_t *sa, size_t *sb,
+                                                 size_t &tot_a, size_t &tot_b) {
+  const int t = threadIdx.x & 31, w = threadIdx.x >> 5;
+  size_t ia = a, ib = b;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const size_t ya = __shfl_up_sync(0xffffffffu, ia, o), yb = __shfl_up_sync(0xffffffffu, ib, o);
+    if (t >= o) {
+      ia += ya;
+      ib += yb;
+    }
+  }
+  if (t == 31) {
+    sa[w] = ia;
+    sb[w] = ib;
+  }
+  __syncthreads();
+  if (w == 0) {
+    size_t xa = t < (int)(blockDim.x >> 5) ? sa[t] : 0, xb = t < (int)(blockDim.x >> 5) ? sb[t] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const size_t ya = __shfl_up_sync(0xffffffffu, xa, o), yb = __shfl_up_sync(0xffffffffu, xb, o);
+      if (t >= o) {
+        xa += ya;
+        xb += yb;
+      }
+    }
+    sa[t] = xa;  // inclusive over warps
+    sb[t] = xb;
+  }
+  __syncthreads();
+  const size_t wa = w ? sa[w - 1] : 0, wb = w ? sb[w - 1] : 0;
+  tot_a = sa[(blockDim.x >> 5) - 1];
+  tot_b = sb[(blockDim.x >> 5) - 1];
+  a = wa + ia - a;
+  b = wb + ib - b;
+}
+
+__global__ void __launch_bounds__(1024) k_scan_local(const uint8_t *bw, const uint16_t *count,
+                                                     size_t n, size_t *off_words, size_t *off_exc,
+                                                     size_t *blk_words, size_t *blk_exc) {
+  __shared__ size_t sa[32], sb[32];
+  const size_t v = (size_t)blockIdx.x * 1024 + threadIdx.x;
+  size_t a = v < n ? (size_t)bw[v] * 16 : 0, b = v < n ? count[v] : 0;
+  size_t ta, tb;
+  block_excl_scan2(a, b, sa, sb, ta, tb);
+  if (v < n) {
+    off_words[v] = a;
+    off_exc[v] = b;
+  }
+  if (threadIdx.x == 0) {
+    blk_words[blockIdx.x] = ta;
+    blk_exc[blockIdx.x] = tb;
+  }
+}
+
+__global__ void __launch_bounds__(1024) k_scan_blocks(size_t nb, size_t *blk_words,
+                                                      size_t *blk_exc, size_t *totals) {
+  __shared__ size_t sa[32], sb[32];
+  size_t carry_a = 0, carry_b = 0;
+  for (size_t base = 0; base < nb; base += 1024) {
+    const size_t i = base + threadIdx.x;
+    size_t a = i < nb ? blk_words[i] : 0, b = i < nb ? blk_exc[i] : 0;
+    size_t ta, tb;
+    block_excl_scan2(a, b, sa, sb, ta, tb);
+    if (i < nb) {
+      blk_words[i] = carry_a + a;
+      blk_exc[i] = carry_b + b;
+    }
+    carry_a += ta;
+    carry_b += tb;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    totals[0] = carry_a;
+    totals[1] = carry_b;
+  }
+}
+
+
+// Packing at the final offsets: one warp per vector.
+__global__ void __launch_bounds__(256) k_alp_pack(const double *__restrict__ vals, size_t n_vecs,
+                                                  EncodeSlots sl, size_t *off_words,
+                                                  size_t *off_exc, const size_t *blk_words,
+                                                  const size_t *blk_exc, uint64_t *packed,
+                                                  double *exc, uint16_t *pos) {
+  extern __shared__ __align__(16) double s_vec[];  // 1024 doubles per warp
+  double *sv = s_vec + (threadIdx.x >> 5) * VEC;
   const int t = threadIdx.x & 31;
   const size_t nw = ((size_t)gridDim.x * blockDim.x) >> 5;
   for (size_t v = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n_vecs; v += nw) {
-    const int nwd = sl.bw[v] * 16;
-    const uint64_t *src = sl.packed + v * VEC;
-    uint64_t *dst = packed + off_words[v];
-    for (int i = t; i < nwd; i += 32) dst[i] = src[i];
-    const int c = sl.count[v];
-    for (int i = t; i < c; i += 32) {
-      exc[off_exc[v] + i] = sl.exc[v * VEC + i];
-      pos[off_exc[v] + i] = sl.pos[v * VEC + i];
+    const size_t ow = off_words[v] + blk_words[v >> 10], oe = off_exc[v] + blk_exc[v >> 10];
+    // the vector into shared memory: all of its loads in flight at once
+    const double2 *src = reinterpret_cast<const double2 *>(vals + v * VEC);
+    double2 *dst = reinterpret_cast<double2 *>(sv);
+    __syncwarp();
+#pragma unroll
+    for (int i = 0; i < VEC / 64; ++i) dst[t + 32 * i] = src[t + 32 * i];
+    __syncwarp();
+    if (t == 0) {
+      off_words[v] = ow;  // the column's final offsets
+      off_exc[v] = oe;
     }
+    pack_vector(sv, sl.exp[v], sl.fac[v], t, sl.fill[v], sl.base[v], sl.bw[v], packed + ow,
+                exc + oe, pos + oe);
   }
 }
 
@@ -390,9 +597,34 @@ flsgpu_status run_alp_encode(const double *vals, size_t n_vecs, int mode, const 
                              size_t *off_exc, size_t *totals, uint64_t *packed, double *exc,
                              uint16_t *pos, cudaStream_t s) {
   if (!n_vecs) return FLSGPU_OK;
-  k_alp_encode<<<warps_grid(n_vecs), 256, 0, s>>>(vals, n_vecs, mode, cand, k_cand, max_exc, sl);
-  k_scan_sizes<<<1, 1024, 0, s>>>(sl.bw, sl.count, n_vecs, off_words, off_exc, totals);
-  k_compact<<<warps_grid(n_vecs), 256, 0, s>>>(sl, n_vecs, off_words, off_exc, packed, exc, pos);
+  if (mode == 1) {
+    flsgpu_status st = check_cuda(cudaMemsetAsync(sl.fb_count, 0, sizeof(uint32_t), s), "memset");
+    if (st) return st;
+  }
+  k_alp_choose<<<warps_grid(n_vecs), 256, 0, s>>>(vals, n_vecs, mode, cand, k_cand, max_exc, sl);
+  if (mode == 1) {
+    k_alp_fallback<<<warps_grid(n_vecs), 256, 0, s>>>(vals, sl);
+    note_launch();
+  }
+  const size_t nb = (n_vecs + 1023) / 1024;
+  k_scan_local<<<(unsigned)nb, 1024, 0, s>>>(sl.bw, sl.count, n_vecs, off_words, off_exc,
+                                             sl.blk_words, sl.blk_exc);
+  k_scan_blocks<<<1, 1024, 0, s>>>(nb, sl.blk_words, sl.blk_exc, totals);
+  note_launch();
+  {
+    flsgpu_status st = check_cuda(cudaMemsetAsync(totals + 2, 0, 3 * sizeof(size_t), s), "memset");
+    if (st) return st;
+  }
+  k_encode_stats<<<persistent_blocks(n_vecs / 32 + 1, 8, 2), 256, 0, s>>>(sl.flags, sl.bw, n_vecs,
+                                                                           totals);
+  note_launch();
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_alp_pack, cudaFuncAttributeMaxDynamicSharedMemorySize, 8 * VEC * 8);
+    attr = true;
+  }
+  k_alp_pack<<<warps_grid(n_vecs), 256, 8 * VEC * sizeof(double), s>>>(
+      vals, n_vecs, sl, off_words, off_exc, sl.blk_words, sl.blk_exc, packed, exc, pos);
   note_launch(3);
   return check_cuda(cudaGetLastError(), "alp encode");
 }

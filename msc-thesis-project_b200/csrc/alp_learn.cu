@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "alp_learn.cuh"
+#include "umma.cuh"
 
 namespace flsb200 {
 
@@ -45,17 +46,20 @@ __device__ __forceinline__ float warp_max_f(float x) {
 // fractions, histograms of the decimal digits after the point (smallest d
 // with x * 10^d integral), of trailing zero bits of the mantissa, of
 // log10|x|, and of the binary exponent.
-__global__ void __launch_bounds__(256) k_features(const double *__restrict__ vals, size_t n_vecs,
-                                                  __nv_bfloat16 *feat) {
-  const int t = threadIdx.x & 31;
-  const size_t nw = ((size_t)gridDim.x * blockDim.x) >> 5;
-  for (size_t v = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n_vecs; v += nw) {
-    const double x = vals[v * VEC + 32 * t];
+// Lane t receives features t and t + 32 (lo, hi); x is the lane's sample.
+__device__ __forceinline__ void vector_features(double x, int t, float &lo_out, float &hi_out) {
+  {
     const uint64_t bits = (uint64_t)__double_as_longlong(x);
     const bool fin = isfinite(x);
     const double a = fabs(x);
     const bool nz = fin && a > 0.0;
-    const float l = nz ? (float)log10(a) : 0.0f;
+    // log10|x| from the binary exponent and the mantissa in [1, 2) (single
+    // precision is far finer than the bf16 features; subnormals in double)
+    const int ef = (int)((bits >> 52) & 0x7FF);
+    const float mant = __uint_as_float(0x3F800000u | (uint32_t)((bits >> 29) & 0x7FFFFFu));
+    const float l = !nz ? 0.0f
+                        : ef ? __log10f(mant) + (float)(ef - 1023) * 0.30102999566f
+                             : (float)log10(a);
     int d = 17;
     if (fin) {
       for (int dd = 0; dd < 17; ++dd) {
@@ -113,9 +117,291 @@ __global__ void __launch_bounds__(256) k_features(const double *__restrict__ val
         hi = f[j + 32];
       }
     }
+    lo_out = lo;
+    hi_out = hi;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_features(const double *__restrict__ vals, size_t n_vecs,
+                                                  __nv_bfloat16 *feat) {
+  const int t = threadIdx.x & 31;
+  const size_t nw = ((size_t)gridDim.x * blockDim.x) >> 5;
+  for (size_t v = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n_vecs; v += nw) {
+    float lo, hi;
+    vector_features(vals[v * VEC + 32 * t], t, lo, hi);
     feat[v * kFeatures + t] = __float2bfloat16_rn(lo);
     feat[v * kFeatures + 32 + t] = __float2bfloat16_rn(hi);
   }
+}
+
+using bf16 = __nv_bfloat16;
+
+// ---- fused inference ------------------------------------------------------
+// Features -> three layers -> top-k candidates of 128 vectors per step in
+// one persistent kernel (16 warps, one CTA per SM).  The bf16 weights are
+// staged once per CTA in shared memory in the canonical K-major layout.  Per
+// tile (row r = vector m0 + r): each warp computes the features of 8 rows
+// into the activation tile; one thread issues the MMAs of a layer
+// (tcgen05, FP32 accumulators in tensor memory: layers 1 and 3 at columns
+// 0.., layer 2 at 128..); warp w reads back tensor-memory lanes 32 (w % 4)
+// .. +31 (those rows) for column quarter w / 4, adding bias + ReLU into the
+// next activation tile, or, after layer 3, keeping the top-k of its quarter
+// of the logits, which warps 0..3 merge per row.  The arithmetic is the
+// layer-by-layer path's (the same MMAs in the same K order, bf16
+// activations, fp32 logits, ties to the lower class), so the candidates are
+// the same.
+constexpr int kPropRows = 128;
+constexpr int kPropThreads = 512;
+constexpr int kTopMax = 4;
+constexpr size_t kPropSmem =
+    (size_t)(kHidden * kFeatures + kHidden * kHidden + kOut * kHidden + kPropRows * kHidden) * 2 +
+    (size_t)(kHidden + kHidden + kOut) * 4 + (size_t)4 * kPropRows * kTopMax * (4 + 4);
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+      "%14,%15}, [%16];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;");
+}
+
+// Issues the K/16 MMAs of one layer: D[tmem] = A (128 x K, canonical, sA) .
+// B (N x K, canonical, sB)^T, then commits them to the mbarrier.
+__device__ __forceinline__ void issue_layer(uint32_t tmem_d, uint32_t sA, uint32_t sB, int N, int K,
+                                            uint64_t *mbar) {
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t idesc = umma_idesc_bf16(kPropRows, N);
+  const uint32_t lbo_a = (kPropRows / 8) * 128, lbo_b = (uint32_t)(N / 8) * 128;
+  for (int s = 0; s < K / 16; ++s) {
+    const uint64_t da = umma_desc(sA + s * 2 * lbo_a, lbo_a, 128);
+    const uint64_t db = umma_desc(sB + s * 2 * lbo_b, lbo_b, 128);
+    const uint32_t acc = s > 0 ? 1u : 0u;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(da), "l"(db), "r"(idesc), "r"(acc));
+  }
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+      smem_u32(mbar)));
+}
+
+// Columns [32 q, 32 q + 32) of the row's hidden accumulator at tmem_col +
+// bias, ReLU, to bf16 in the activation tile (K = 128 canonical layout).
+__device__ __forceinline__ void hidden_epilogue(uint32_t tmem, int lanes, int q, int row,
+                                                uint32_t tmem_col, const float *bias,
+                                                unsigned char *sA) {
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int c0 = 32 * q + 16 * h;
+    uint32_t r[16];
+    tmem_ld16(tmem + ((uint32_t)lanes << 16) + tmem_col + (uint32_t)c0, r);
+    uint32_t packed[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const float a = fmaxf(__uint_as_float(r[2 * j]) + bias[c0 + 2 * j], 0.0f);
+      const float b = fmaxf(__uint_as_float(r[2 * j + 1]) + bias[c0 + 2 * j + 1], 0.0f);
+      const __nv_bfloat162 hv = __floats2bfloat162_rn(a, b);
+      packed[j] = *reinterpret_cast<const uint32_t *>(&hv);
+    }
+    *reinterpret_cast<uint4 *>(sA + canon_off(row, c0, kPropRows)) =
+        make_uint4(packed[0], packed[1], packed[2], packed[3]);
+    *reinterpret_cast<uint4 *>(sA + canon_off(row, c0 + 8, kPropRows)) =
+        make_uint4(packed[4], packed[5], packed[6], packed[7]);
+  }
+}
+
+// Insertion into a list sorted by descending value; a value equal to one
+// already listed goes behind it (candidates arrive in ascending class).
+__device__ __forceinline__ void top_insert(float (&bv)[kTopMax], int (&bc)[kTopMax], int k, float val,
+                                           int cls) {
+#pragma unroll
+  for (int q = 0; q < kTopMax; ++q) {
+    if (q < k && cls >= 0 && (bc[q] < 0 || val > bv[q])) {
+      const float tv = bv[q];
+      const int tc = bc[q];
+      bv[q] = val;
+      bc[q] = cls;
+      val = tv;
+      cls = tc;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kPropThreads, 1)
+    k_propose(const double *__restrict__ vals, size_t n_vecs, const bf16 *__restrict__ w1,
+              const bf16 *__restrict__ w2, const bf16 *__restrict__ w3,
+              const float *__restrict__ b1, const float *__restrict__ b2,
+              const float *__restrict__ b3, int k, int16_t *cand, uint32_t *status) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t tmem_slot;
+  unsigned char *sW1 = smem;
+  unsigned char *sW2 = sW1 + kHidden * kFeatures * 2;
+  unsigned char *sW3 = sW2 + kHidden * kHidden * 2;
+  unsigned char *sA = sW3 + kOut * kHidden * 2;
+  float *sb1 = reinterpret_cast<float *>(sA + kPropRows * kHidden * 2);
+  float *sb2 = sb1 + kHidden;
+  float *sb3 = sb2 + kHidden;
+  float *s_topv = sb3 + kOut;                                         // [4][128][kTopMax]
+  int *s_topc = reinterpret_cast<int *>(s_topv + 4 * kPropRows * kTopMax);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int lanes = 32 * (warp & 3), quarter = warp >> 2, row = lanes + lane;
+  constexpr uint32_t kCols = 256;
+
+  // weights and biases, once per CTA
+  for (int i = tid; i < kHidden * kFeatures / 8; i += kPropThreads) {
+    const int r = i / (kFeatures / 8), kg = i % (kFeatures / 8);
+    *reinterpret_cast<uint4 *>(sW1 + canon_off(r, kg * 8, kHidden)) =
+        *reinterpret_cast<const uint4 *>(w1 + (size_t)r * kFeatures + kg * 8);
+  }
+  for (int i = tid; i < kHidden * kHidden / 8; i += kPropThreads) {
+    const int r = i / (kHidden / 8), kg = i % (kHidden / 8);
+    *reinterpret_cast<uint4 *>(sW2 + canon_off(r, kg * 8, kHidden)) =
+        *reinterpret_cast<const uint4 *>(w2 + (size_t)r * kHidden + kg * 8);
+  }
+  for (int i = tid; i < kOut * kHidden / 8; i += kPropThreads) {
+    const int r = i / (kHidden / 8), kg = i % (kHidden / 8);
+    *reinterpret_cast<uint4 *>(sW3 + canon_off(r, kg * 8, kOut)) =
+        *reinterpret_cast<const uint4 *>(w3 + (size_t)r * kHidden + kg * 8);
+  }
+  for (int i = tid; i < kHidden; i += kPropThreads) {
+    sb1[i] = b1[i];
+    sb2[i] = b2[i];
+  }
+  for (int i = tid; i < kOut; i += kPropThreads) sb3[i] = b3[i];
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&tmem_slot)),
+                 "r"(kCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&mbar)), "r"(1));
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = tmem_slot;
+  const uint32_t aA = smem_u32(sA), aW1 = smem_u32(sW1), aW2 = smem_u32(sW2), aW3 = smem_u32(sW3);
+  uint32_t phase = 0;
+  bool failed = false;
+  const size_t n_tiles = (n_vecs + kPropRows - 1) / kPropRows;
+  constexpr int kRowsPerWarp = kPropRows / (kPropThreads / 32);  // 8
+
+  for (size_t tile = blockIdx.x; tile < n_tiles && !failed; tile += gridDim.x) {
+    const size_t m0 = tile * kPropRows;
+    // features of this warp's 8 rows: lane j loads sample j of all of them
+    // first (one round trip), then the warp works through them
+    double xs[kRowsPerWarp];
+#pragma unroll
+    for (int i = 0; i < kRowsPerWarp; ++i) {
+      const size_t v = m0 + warp * kRowsPerWarp + i;
+      xs[i] = v < n_vecs ? vals[v * VEC + 32 * lane] : 0.0;
+    }
+#pragma unroll
+    for (int i = 0; i < kRowsPerWarp; ++i) {
+      float lo, hi;
+      vector_features(xs[i], lane, lo, hi);
+      const int r = warp * kRowsPerWarp + i;
+      *reinterpret_cast<bf16 *>(sA + canon_off(r, lane, kPropRows)) = __float2bfloat16_rn(lo);
+      *reinterpret_cast<bf16 *>(sA + canon_off(r, lane + 32, kPropRows)) = __float2bfloat16_rn(hi);
+    }
+    asm volatile("fence.proxy.async.shared::cta;");
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    // layer 1 -> columns 0..127
+    if (tid == 0) issue_layer(tmem, aA, aW1, kHidden, kFeatures, &mbar);
+    if (__syncthreads_or(!mbar_wait(&mbar, phase))) {
+      failed = true;
+      break;
+    }
+    phase ^= 1u;
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    hidden_epilogue(tmem, lanes, quarter, row, 0, sb1, sA);
+    asm volatile("fence.proxy.async.shared::cta;");
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    // layer 2 -> columns 128..255
+    if (tid == 0) issue_layer(tmem + 128, aA, aW2, kHidden, kHidden, &mbar);
+    if (__syncthreads_or(!mbar_wait(&mbar, phase))) {
+      failed = true;
+      break;
+    }
+    phase ^= 1u;
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    hidden_epilogue(tmem, lanes, quarter, row, 128, sb2, sA);
+    asm volatile("fence.proxy.async.shared::cta;");
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    // layer 3 -> columns 0..191
+    if (tid == 0) issue_layer(tmem, aA, aW3, kOut, kHidden, &mbar);
+    if (__syncthreads_or(!mbar_wait(&mbar, phase))) {
+      failed = true;
+      break;
+    }
+    phase ^= 1u;
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    // top-k of this quarter of the row's logits (classes 48 q .. 48 q + 47;
+    // class 191 is padding)
+    {
+      float bv[kTopMax];
+      int bc[kTopMax];
+#pragma unroll
+      for (int q = 0; q < kTopMax; ++q) {
+        bv[q] = -INFINITY;
+        bc[q] = -1;
+      }
+#pragma unroll
+      for (int h = 0; h < 3; ++h) {
+        const int c0 = 48 * quarter + 16 * h;
+        uint32_t r[16];
+        tmem_ld16(tmem + ((uint32_t)lanes << 16) + (uint32_t)c0, r);
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int c = c0 + j;
+          if (c < kClasses) top_insert(bv, bc, k, __uint_as_float(r[j]) + sb3[c], c);
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < kTopMax; ++q) {
+        s_topv[(quarter * kPropRows + row) * kTopMax + q] = bv[q];
+        s_topc[(quarter * kPropRows + row) * kTopMax + q] = bc[q];
+      }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if (quarter == 0) {
+      // merge the quarters in class order: a logit equal to one already
+      // listed stays behind it
+      float bv[kTopMax];
+      int bc[kTopMax];
+#pragma unroll
+      for (int q = 0; q < kTopMax; ++q) {
+        bv[q] = s_topv[row * kTopMax + q];
+        bc[q] = s_topc[row * kTopMax + q];
+      }
+      for (int qq = 1; qq < 4; ++qq)
+#pragma unroll
+        for (int q = 0; q < kTopMax; ++q)
+          top_insert(bv, bc, k, s_topv[(qq * kPropRows + row) * kTopMax + q],
+                     s_topc[(qq * kPropRows + row) * kTopMax + q]);
+      const size_t v = m0 + row;
+      if (v < n_vecs)
+        for (int q = 0; q < k; ++q) cand[v * k + q] = (int16_t)bc[q];
+    }
+    // the activation tile, the top-k scratch and tensor memory are reused
+    __syncthreads();
+  }
+  if (failed) {
+    if (tid == 0 && status) atomicOr(status, 0x100u);
+    mbar_wait(&mbar, phase);  // the MMAs in flight, bounded, before dealloc
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols));
 }
 
 // Softmax cross entropy over the 191 real classes of each row (class 191
@@ -329,8 +615,10 @@ flsgpu_status ensure_rows(flsgpu_alp_encoder *e, int rows) {
 }
 
 void free_enc(flsgpu_alp_encoder *e) {
-  for (void *p : {(void *)e->feat, (void *)e->labels, (void *)e->cand, (void *)e->sl.packed,
-                  (void *)e->sl.exc, (void *)e->sl.pos, (void *)e->sl.bw, (void *)e->sl.base,
+  for (void *p : {(void *)e->feat, (void *)e->labels, (void *)e->cand, (void *)e->sl.fill,
+                  (void *)e->sl.fb_list, (void *)e->sl.fb_count, (void *)e->sl.blk_words,
+                  (void *)e->sl.blk_exc,
+                  (void *)e->sl.bw, (void *)e->sl.base,
                   (void *)e->sl.fac, (void *)e->sl.exp, (void *)e->sl.count, (void *)e->sl.flags,
                   (void *)e->off_words, (void *)e->off_exc, (void *)e->totals, (void *)e->packed,
                   (void *)e->exc, (void *)e->pos})
@@ -353,9 +641,11 @@ flsgpu_status ensure_vecs(flsgpu_alp_encoder *e, size_t n_vecs) {
   e->feat = dalloc<bf16>(n * kFeatures, st);
   e->labels = dalloc<int16_t>(n, st);
   e->cand = dalloc<int16_t>(n * 4, st);
-  e->sl.packed = dalloc<uint64_t>(n * VEC, st);
-  e->sl.exc = dalloc<double>(n * VEC, st);
-  e->sl.pos = dalloc<uint16_t>(n * VEC, st);
+  e->sl.fill = dalloc<int64_t>(n, st);
+  e->sl.fb_list = dalloc<uint32_t>(n, st);
+  e->sl.fb_count = dalloc<uint32_t>(1, st);
+  e->sl.blk_words = dalloc<size_t>(n / 1024 + 1, st);
+  e->sl.blk_exc = dalloc<size_t>(n / 1024 + 1, st);
   e->sl.bw = dalloc<uint8_t>(n, st);
   e->sl.base = dalloc<uint64_t>(n, st);
   e->sl.fac = dalloc<uint8_t>(n, st);
@@ -364,7 +654,7 @@ flsgpu_status ensure_vecs(flsgpu_alp_encoder *e, size_t n_vecs) {
   e->sl.flags = dalloc<uint8_t>(n, st);
   e->off_words = dalloc<size_t>(n, st);
   e->off_exc = dalloc<size_t>(n, st);
-  e->totals = dalloc<size_t>(4, st);
+  e->totals = dalloc<size_t>(8, st);
   e->packed = dalloc<uint64_t>(n * VEC, st);
   e->exc = dalloc<double>(n * VEC, st);
   e->pos = dalloc<uint16_t>(n * VEC, st);
@@ -471,8 +761,29 @@ flsgpu_status features(const double *vals, size_t n_vecs, bf16 *feat, cudaStream
   return check_cuda(cudaGetLastError(), "k_features");
 }
 
+// The proposals in one fused launch (k_propose).
 flsgpu_status propose(flsgpu_alp_encoder *e, const double *vals, size_t n_vecs, int k,
                       cudaStream_t s) {
+  if (!n_vecs) return FLSGPU_OK;
+  static bool attr = false;
+  if (!attr) {
+    flsgpu_status st = check_cuda(
+        cudaFuncSetAttribute(k_propose, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPropSmem),
+        "k_propose attribute");
+    if (st) return st;
+    attr = true;
+  }
+  const size_t tiles = (n_vecs + kPropRows - 1) / kPropRows;
+  const unsigned grid = (unsigned)std::min<size_t>(tiles, (size_t)sm_count());
+  k_propose<<<grid, kPropThreads, kPropSmem, s>>>(vals, n_vecs, e->w1b, e->w2b, e->w3b, e->w + kOffB1,
+                                               e->w + kOffB2, e->w + kOffB3, k, e->cand, e->status);
+  note_launch();
+  return check_cuda(cudaGetLastError(), "k_propose launch");
+}
+
+// The same proposals layer by layer: features, three GEMM launches, top-k.
+flsgpu_status propose_layered(flsgpu_alp_encoder *e, const double *vals, size_t n_vecs, int k,
+                              cudaStream_t s) {
   flsgpu_status st;
   if ((st = features(vals, n_vecs, e->feat, s))) return st;
   const int chunk = 1 << 16;
@@ -678,6 +989,22 @@ flsgpu_status flsgpu_alp_encoder_propose(flsgpu_alp_encoder *e, const double *d_
   return st;
 }
 
+// The layer-by-layer path of the same proposals (features, three GEMM
+// launches, top-k): kept so that tests can hold the fused kernel to it.
+flsgpu_status flsgpu_alp_encoder_propose_layered(flsgpu_alp_encoder *e, const double *d_values,
+                                                 size_t n_values, uint32_t k, int16_t *d_cand,
+                                                 flsgpu_stream stream) {
+  if (!e || !d_values || (n_values % VEC) || k < 1 || k > 4)
+    return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "propose: bad arguments");
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t n_vecs = n_values / VEC;
+  flsgpu_status st = ensure_vecs(e, n_vecs);
+  if (!st) st = propose_layered(e, d_values, n_vecs, (int)k, s);
+  if (!st && d_cand)
+    st = check_cuda(cudaMemcpyAsync(d_cand, e->cand, sizeof(int16_t) * n_vecs * k, cudaMemcpyDeviceToDevice, s), "copy");
+  return st;
+}
+
 flsgpu_status flsgpu_alp_encoder_save(const flsgpu_alp_encoder *e, const char *path) {
   if (!e || !path) return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "null argument");
   std::vector<float> h(kParams);
@@ -728,19 +1055,11 @@ flsgpu_status flsgpu_alp_encode_f64(flsgpu_alp_encoder *e, const double *d_value
   if ((st = run_alp_encode(d_values, n_vecs, (int)mode, e->cand, 3, 30, e->sl, e->off_words,
                            e->off_exc, e->totals, e->packed, e->exc, e->pos, s)))
     return st;
-  size_t tot[2] = {0, 0};
+  size_t tot[5] = {0, 0, 0, 0, 0};
   if ((st = check_cuda(cudaMemcpyAsync(tot, e->totals, sizeof(tot), cudaMemcpyDeviceToHost, s), "copy")) ||
       (st = check_cuda(cudaStreamSynchronize(s), "sync")))
     return st;
-  std::vector<uint8_t> flags(n_vecs), bws(n_vecs);
-  cudaMemcpy(flags.data(), e->sl.flags, n_vecs, cudaMemcpyDeviceToHost);
-  cudaMemcpy(bws.data(), e->sl.bw, n_vecs, cudaMemcpyDeviceToHost);
-  size_t fb = 0, rd = 0, bwsum = 0;
-  for (size_t i = 0; i < n_vecs; ++i) {
-    fb += flags[i] & 1;
-    rd += (flags[i] >> 1) & 1;
-    bwsum += bws[i];
-  }
+  const size_t fb = tot[2], rd = tot[3], bwsum = tot[4];
   std::memset(out, 0, sizeof(*out));
   flsgpu_alp_column &c = out->column;
   c.n_values = n_values;

@@ -29,26 +29,28 @@ __host__ __device__ inline int class_fac(int c) {
   return c - e * (e + 1) / 2;
 }
 
-// Per-vector encode results in fixed slots (1024 entries per vector), before
-// compaction into the contiguous column.
+// Per-vector encode parameters and sizes (the column's metadata arrays, plus
+// the fill integer and the flags).
 struct EncodeSlots {
-  uint64_t *packed;   // n_vecs * 1024 words
-  double *exc;        // n_vecs * 1024
-  uint16_t *pos;      // n_vecs * 1024
   uint8_t *bw;
   uint64_t *base;
+  int64_t *fill;      // integer stored at exception positions
   uint8_t *fac;
   uint8_t *exp;
   uint16_t *count;
-  uint8_t *flags;     // 1 = the proposal fell back to the plain search
+  uint8_t *flags;     // 1 = the proposal fell back to the plain search; 2 = ALP-RD
+  uint32_t *fb_list;  // vectors whose proposal fell back (mode 1)
+  uint32_t *fb_count;
+  size_t *blk_words;  // per 1024 vectors: offsets of the scan's blocks
+  size_t *blk_exc;
 };
 
 // Launchers (alp_encode.cu)
 flsgpu_status run_plain_labels(const double *vals, size_t n_vecs, int16_t *labels, int32_t *est,
                                cudaStream_t s);
-// encode (mode 0: plain search; 1: verified proposals with fallback), then
-// scan of the per-vector sizes (totals[0] = packed words, totals[1] =
-// exceptions) and compaction into packed / exc / pos
+// parameter choice (mode 0: plain search; 1: verified proposals with
+// fallback) and analysis, scan of the per-vector sizes (totals[0] = packed
+// words, totals[1] = exceptions), then packing into packed / exc / pos
 flsgpu_status run_alp_encode(const double *vals, size_t n_vecs, int mode, const int16_t *cand,
                              int k_cand, int max_exc, const EncodeSlots &sl, size_t *off_words,
                              size_t *off_exc, size_t *totals, uint64_t *packed, double *exc,

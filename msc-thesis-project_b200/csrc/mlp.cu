@@ -18,42 +18,12 @@
 #include <vector>
 
 #include "alp_learn.cuh"
+#include "umma.cuh"
 
 namespace flsb200 {
 
 constexpr int kGemmThreads = 128;
 constexpr int kKChunk = 64;
-constexpr uint32_t kSpinLimit = 1u << 26;  // bounded mbarrier wait
-
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-// UMMA shared-memory descriptor, no swizzle, K-major (bit layout as CUTLASS
-// cute::UMMA::SmemDescriptor: start >>4 [0,14), LBO >>4 [16,30), SBO >>4
-// [32,46), version 1 [46,48), layout type 0 [61,64)).
-__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
-  uint64_t d = 0;
-  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
-  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
-  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
-  d |= (uint64_t)1 << 46;
-  return d;
-}
-
-// Instruction descriptor for kind::f16: F32 accumulator (bits 4-5 = 1),
-// A and B BF16 (bits 7-9, 10-12 = 1), both K-major, N >> 3 at bit 17,
-// M >> 4 at bit 24.
-__host__ __device__ constexpr uint32_t umma_idesc_bf16(int M, int N) {
-  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) |
-         ((uint32_t)(M >> 4) << 24);
-}
-
-// byte offset of element (r, k) of a tile of R rows x 64 K in the canonical
-// no-swizzle K-major layout
-__device__ __forceinline__ uint32_t canon_off(int r, int k, int R) {
-  return (uint32_t)((((k >> 3) * (R >> 3) + (r >> 3)) << 7) + ((r & 7) << 4) + ((k & 7) << 1));
-}
 
 __global__ void __launch_bounds__(kGemmThreads) k_gemm_tn(const GemmArgs g) {
   extern __shared__ __align__(128) unsigned char smem[];

@@ -688,12 +688,14 @@ class AlpEncoder:
                                            P(_stream_handle(stream))))
         return r
 
-    def propose(self, values, k=3, stream=None):
+    def propose(self, values, k=3, stream=None, layered=False):
+        """Top-k proposed classes per vector (fused kernel; layered=True runs
+        the layer-by-layer launches instead)."""
         torch = _torch()
         cand = torch.empty(values.numel() // 1024 * k, dtype=torch.int16, device=values.device)
-        _check(_fn("flsgpu_alp_encoder_propose")(self.h, P(_ptr(values)), SZ(values.numel()),
-                                                C.c_uint32(k), P(_ptr(cand)),
-                                                P(_stream_handle(stream))))
+        name = "flsgpu_alp_encoder_propose_layered" if layered else "flsgpu_alp_encoder_propose"
+        _check(_fn(name)(self.h, P(_ptr(values)), SZ(values.numel()), C.c_uint32(k),
+                         P(_ptr(cand)), P(_stream_handle(stream))))
         return cand.view(-1, k)
 
     def params(self) -> np.ndarray:

@@ -176,3 +176,18 @@ def test_training_and_learned_encoder(cuda, tmp_path):
     enc2 = F.AlpEncoder(seed=9)
     enc2.load(str(p))
     assert np.array_equal(enc.params(), enc2.params())
+
+
+def test_fused_proposal_matches_layered(cuda):
+    """The fused proposal kernel (features, three tcgen05 layers and top-k in
+    one launch) gives the classes of the layer-by-layer launches, on a
+    column whose last 128-vector tile is partial."""
+    import torch
+    enc = F.AlpEncoder(seed=4)
+    enc.train(torch.from_numpy(colgen.learned_values(41, 2048)).to(cuda), epochs=2, batch=1024,
+              lr=3e-3)
+    vals = torch.from_numpy(colgen.learned_values(42, 1000)).to(cuda)
+    for k in (1, 3, 4):
+        fused = enc.propose(vals, k)
+        layered = enc.propose(vals, k, layered=True)
+        assert torch.equal(fused, layered), k
