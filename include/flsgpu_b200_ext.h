@@ -75,6 +75,33 @@ flsgpu_status flsgpu_tuning_get_variant(uint32_t type, uint32_t kind, uint32_t *
 flsgpu_status flsgpu_tuning_set_prefetch(uint32_t lane_bits, const uint64_t mask[2]);
 flsgpu_status flsgpu_tuning_get_prefetch(uint32_t lane_bits, uint64_t mask[2]);
 
+/* ---- decode of host-resident columns, pipelined (the reference's host
+ *      binding copies a whole column in, decodes, synchronises and copies
+ *      back: src/engine/kernels.cuh:94-112) ---------------------------------
+ * The column descriptor holds HOST pointers (pin them for asynchronous,
+ * full-speed copies); the decoded values land in host_out.  Chunks of
+ * chunk_values values (a multiple of 1024) are copied in, decoded and
+ * copied out on three streams over double-buffered device staging that the
+ * pipeline allocates once (about 34 bytes per chunk value per slot), so
+ * copies in both directions overlap the decode.  factors / fractions may
+ * be host tables or NULL.  Each call returns when host_out is complete;
+ * calls on one pipeline must not overlap. */
+typedef struct flsgpu_host_pipeline flsgpu_host_pipeline;
+flsgpu_status flsgpu_host_pipeline_create(size_t chunk_values, flsgpu_host_pipeline **out);
+void flsgpu_host_pipeline_destroy(flsgpu_host_pipeline *pipeline);
+flsgpu_status flsgpu_host_decompress_ffor_u32(flsgpu_host_pipeline *pipeline,
+                                              const flsgpu_ffor_column *host_column,
+                                              uint32_t *host_out, const flsgpu_decode_opts *opts);
+flsgpu_status flsgpu_host_decompress_ffor_u64(flsgpu_host_pipeline *pipeline,
+                                              const flsgpu_ffor_column *host_column,
+                                              uint64_t *host_out, const flsgpu_decode_opts *opts);
+flsgpu_status flsgpu_host_decompress_alp_f32(flsgpu_host_pipeline *pipeline,
+                                             const flsgpu_alp_column *host_column,
+                                             float *host_out, const flsgpu_decode_opts *opts);
+flsgpu_status flsgpu_host_decompress_alp_f64(flsgpu_host_pipeline *pipeline,
+                                             const flsgpu_alp_column *host_column,
+                                             double *host_out, const flsgpu_decode_opts *opts);
+
 /* ---- fused pair query over compressed columns (no reference counterpart)
  * For each pair i: d_results[i] = sum of A_i[k] over positions k with
  * B_i[k] < median(B_i), where A_i is an f64 ALP column, B_i a u32 FFOR

@@ -370,6 +370,39 @@ def launch_count() -> int:
 
 
 # ---------------------------------------------------------------------------
+# host-resident columns, pipelined decode
+# ---------------------------------------------------------------------------
+def host_ffor_column(packed, bit_widths, offsets, bases, n_values: int) -> tuple:
+    """An FFOR descriptor over host (CPU, ideally pinned) torch tensors;
+    returns (descriptor, kind, dtype, tensors kept alive)."""
+    bits = packed.element_size() * 8
+    n_vecs = (n_values + 1023) // 1024
+    bp = BPColumnC(n_values, n_vecs, packed.data_ptr(), bit_widths.data_ptr(), offsets.data_ptr())
+    c = FFORColumnC(n_values, bp, bases.data_ptr())
+    return c, "ffor", f"u{bits}", (packed, bit_widths, offsets, bases)
+
+
+class HostPipeline:
+    """Pipelined decode of host-resident columns into host memory
+    (flsgpu_host_*): chunks of chunk_values values are copied in, decoded
+    and copied out on three streams."""
+
+    def __init__(self, chunk_values: int = 1 << 20):
+        self.h = P()
+        _check(_fn("flsgpu_host_pipeline_create")(SZ(chunk_values), C.byref(self.h)))
+
+    def decompress(self, desc, kind: str, dtype: str, host_out, o: DecodeOpts | None = None):
+        _check(_fn(f"flsgpu_host_decompress_{kind}_{dtype}")(
+            self.h, C.byref(desc), P(host_out.data_ptr()), C.byref(o) if o is not None else None))
+        return host_out
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().flsgpu_host_pipeline_destroy(self.h)
+            self.h = None
+
+
+# ---------------------------------------------------------------------------
 # decode tuning and the autotuner
 # ---------------------------------------------------------------------------
 TYPE_CODES = {"u32": 0, "u64": 1, "f32": 2, "f64": 3}
