@@ -666,7 +666,7 @@ def run_e2e(args, dev):
     import torch
     import flsgpu_b200 as F
     rng = np.random.default_rng(7)
-    pipe = F.HostPipeline(chunk_values=1 << 20)
+    pipe = F.HostPipeline(chunk_values=1 << 22)
     jobs = []
     for bits, n_values, widths in ((32, 2 ** 24, (1, 7, 16, 32)), (64, 2 ** 23, (1, 20, 40, 64))):
         n_vecs = n_values // 1024
@@ -705,7 +705,7 @@ def run_e2e(args, dev):
             "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
             "ms_per_step": round(ms, 3),
             "sample": "u32 2^24 values x w{1,7,16,32} + u64 2^23 x w{1,20,40,64}, pinned host "
-                      "buffers, flsgpu_host_decompress_ffor_* (chunks of 2^20 values, copies "
+                      "buffers, flsgpu_host_decompress_ffor_* (chunks of 2^22 values, copies "
                       "overlapping the decode), host clock around synchronous calls"}
 
 
@@ -893,7 +893,10 @@ def main():
                              "unit": "GB/s", "frac": round(r["achieved"] / hbm, 4),
                              "peak_kind": pk_kind,
                              "kernel": "k_store<f64/f32, ALP> and k_alprd<f64>",
-                             "traffic": None},
+                             "algorithmic_bytes_per_launch": round(r["bytes_step"] / 3),
+                             "traffic": profiled_traffic("alp_decode_at_scale.md",
+                                                         r["bytes_step"] / 3),
+                             "traffic_source": "profiles/alp_decode_at_scale.md (ncu, one pass)"},
                 "gpu_launches": r["launches"], "clocks": r["clocks"],
                 "generation_s": round(r["gen_s"], 1)}))
         return

@@ -387,7 +387,7 @@ class HostPipeline:
     (flsgpu_host_*): chunks of chunk_values values are copied in, decoded
     and copied out on three streams."""
 
-    def __init__(self, chunk_values: int = 1 << 20):
+    def __init__(self, chunk_values: int = 1 << 22):
         self.h = P()
         _check(_fn("flsgpu_host_pipeline_create")(SZ(chunk_values), C.byref(self.h)))
 
