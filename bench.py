@@ -151,13 +151,21 @@ def barrier(world):
 
 
 def max_over_ranks(x: float, world: int) -> float:
+    """The largest of the ranks' values (the slowest replica's time)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def job_gbs(bytes_per_replica_step: int, steps: int, world: int, max_ms: float) -> float:
+    """Whole-job GB/s of `world` replicas each moving bytes_per_replica_step
+    per step, timed by the slowest replica."""
+    return bytes_per_replica_step * steps * world / (max_ms / 1e3) / 1e9
 
 
 # ---------------------------------------------------------------------------
@@ -259,7 +267,7 @@ def run_ffor(args, rank, world, dev):
     read_b = total_read if not fsum else total_read
     write_b = total_write if not fsum else 8 * len(cols)
     bytes_step = read_b + write_b
-    gbs = bytes_step * args.steps * world / (ms / 1e3) / 1e9
+    gbs = job_gbs(bytes_step, args.steps, world, ms)
     per_width = {"u32": [], "u64": []}
     for (bits, w, c), t in zip(cols, per_col_ms):
         r, wr = col_bytes(c)
