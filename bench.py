@@ -668,7 +668,7 @@ def run_e2e(args, dev):
     step every column's packed words and metadata go from pinned host memory
     to the device and the decoded values come back, chunk by chunk on three
     streams (copies in both directions overlap the decode).  Sample: one u32
-    column of 2^24 values for w in {1, 7, 16, 32} and one u64 column of 2^23
+    column of 2^26 values for w in {1, 7, 16, 32} and one u64 column of 2^25
     values for w in {1, 20, 40, 64}.  Timed on the host clock around whole
     synchronous calls (the pipeline's streams are the library's own)."""
     import torch
@@ -676,7 +676,7 @@ def run_e2e(args, dev):
     rng = np.random.default_rng(7)
     pipe = F.HostPipeline(chunk_values=1 << 22)
     jobs = []
-    for bits, n_values, widths in ((32, 2 ** 24, (1, 7, 16, 32)), (64, 2 ** 23, (1, 20, 40, 64))):
+    for bits, n_values, widths in ((32, 2 ** 26, (1, 7, 16, 32)), (64, 2 ** 25, (1, 20, 40, 64))):
         n_vecs = n_values // 1024
         nl = 1024 // bits
         ut = np.uint64 if bits == 64 else np.uint32
@@ -712,7 +712,7 @@ def run_e2e(args, dev):
     return {"value": round((reads + writes) / (ms / 1e3) / 1e9, 2), "unit": "GB/s",
             "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
             "ms_per_step": round(ms, 3),
-            "sample": "u32 2^24 values x w{1,7,16,32} + u64 2^23 x w{1,20,40,64}, pinned host "
+            "sample": "u32 2^26 values x w{1,7,16,32} + u64 2^25 x w{1,20,40,64}, pinned host "
                       "buffers, flsgpu_host_decompress_ffor_* (chunks of 2^22 values, copies "
                       "overlapping the decode), host clock around synchronous calls"}
 
