@@ -1,15 +1,19 @@
 // decompress_rd.cu -- ALP-RD decoding (the reference has CPU code only:
 // rd_encoder::decode, src/alp/rd.hpp:146-172).
 //
-// Per vector, one warp:
-//   1. unpack the u16 FastLanes left-index lanes (thread t holds lanes 2t
+// Per vector, one warp; all of the vector's loads are issued first (the
+// left index words, the dictionary, the first 32 exceptions, the right
+// parts, which an L2 prefetch one vector earlier has brought close):
+//   1. unpack the right parts (u64 half-lanes / u32 lanes, FFOR base 0) into
+//      shared memory;
+//   2. unpack the u16 FastLanes left-index lanes (thread t holds lanes 2t
 //      and 2t+1 in one 32-bit word per line), look each index up in the
 //      vector's 8-entry dictionary (held one entry per lane, fetched with a
 //      shuffle) and stage the 1024 left parts in shared memory;
-//   2. overwrite the left parts of the exception positions (warp-parallel:
+//   3. overwrite the left parts of the exception positions (warp-parallel:
 //      positions of a vector are distinct);
-//   3. unpack the right parts (u64 half-lanes / u32 lanes, FFOR base 0) and
-//      write (left << right_bw) | right as the output bit pattern.
+//   4. write (left << right_bw) | right as the output bit pattern, 32
+//      consecutive values per warp store.
 #include <cstring>
 
 #include "kernels.cuh"
@@ -57,8 +61,10 @@ template <typename T>
 __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 2 : 1) k_alprd(const RDParams p) {
   using U = typename UintOf<T>::U;
   constexpr int MAXW = sizeof(U) * 8;
-  __shared__ uint16_t s_left_all[8][VEC];
-  uint16_t *sl = s_left_all[threadIdx.x >> 5];
+  extern __shared__ __align__(16) unsigned char rd_smem[];
+  // per warp: the right parts (1024 U) and the left parts (1024 u16)
+  U *sr = reinterpret_cast<U *>(rd_smem) + (threadIdx.x >> 5) * VEC;
+  uint16_t *sl = reinterpret_cast<uint16_t *>(rd_smem + 8 * VEC * sizeof(U)) + (threadIdx.x >> 5) * VEC;
   const int t = threadIdx.x & 31;
   const size_t gw = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const size_t nw = ((size_t)gridDim.x * blockDim.x) >> 5;
@@ -82,20 +88,27 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 2 : 1) k_alprd(const RDP
       if (t == 0 && p.d_status) atomicOr(p.d_status, FLSGPU_BAD_BIT_WIDTH);
       continue;
     }
+    // every load of the vector is issued before any is used: the left
+    // index words, the dictionary entry, the first 32 exceptions, then the
+    // right parts (decoded into shared memory as they arrive)
+    uint32_t lw[16];
+    const uint32_t *lin = reinterpret_cast<const uint32_t *>(p.left_packed + m.loff);
+#pragma unroll
+    for (int j = 0; j < 16; ++j)
+      if (j < m.lbw) lw[j] = ld_stream_u32(lin + j * 32 + t);
     const uint16_t dct = (t < 8) ? p.dicts[8 * (size_t)m.di + t] : 0;
-    // the first 32 exceptions, loaded with the left parts
     uint32_t p0 = VEC;
     uint16_t e0 = 0;
     if ((uint32_t)t < m.cnt) {
       p0 = p.pos[m.eo + t];
       e0 = p.exc[m.eo + t];
     }
-    const uint16_t *lin = p.left_packed + m.loff;
+    const XInt<U> ident{0};
+    decode_values<U, VAR_DEFAULT | VAR_OCC>(right_all + m.roff, m.rbw, t, ident,
+                     [&](int idx, U r, auto...) { sr[idx] = r; });
     switch_width16(m.lbw, [&](auto wc) {
       constexpr int W = decltype(wc)::value;
-      uint32_t wr[W > 0 ? W : 1];
-      load_pair16<W>(lin, t, wr);
-      unpack_pair16<W>(wr, [&](int sub, int k, uint32_t idx) {
+      unpack_pair16<W>(lw, [&](int sub, int k, uint32_t idx) {
         // indices >= 8 only occur at exception positions (patched below)
         const uint16_t left = (uint16_t)__shfl_sync(0xffffffffu, (uint32_t)dct, idx < 8 ? idx : 7);
         sl[(2 * t + sub) + 64 * k] = left;
@@ -118,13 +131,13 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 2 : 1) k_alprd(const RDP
     const size_t rem = p.n_values - vbase;
     const int lim = rem < (size_t)VEC ? (int)rem : VEC;
     U *out = out_all + vbase;
-    const U *rin = right_all + m.roff;
-    const XInt<U> ident{0};
     const int rbw = m.rbw;
-    decode_values<U>(rin, rbw, t, ident, [&](int idx, U r, auto...) {
+#pragma unroll 8
+    for (int i = 0; i < VEC / 32; ++i) {
+      const int idx = t + 32 * i;
       const U l = rbw >= MAXW ? U(0) : (U)((U)sl[idx] << rbw);
-      if (idx < lim) out[idx] = l | r;
-    });
+      if (idx < lim) out[idx] = l | sr[idx];
+    }
     __syncwarp();
   }
 }
@@ -161,14 +174,16 @@ static flsgpu_status decompress_rd(const flsgpu_alprd_column *c, T *d_out,
     return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "null ALP-RD array");
   p.d_status = o ? o->d_status : nullptr;
   p.out = d_out;
+  constexpr size_t smem = 8 * VEC * (sizeof(T) + sizeof(uint16_t));
   static int bps = 0;
   if (bps == 0) {
+    cudaFuncSetAttribute(k_alprd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int b = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_alprd<T>, 256, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_alprd<T>, 256, smem);
     bps = b > 0 ? b : 1;
   }
   const unsigned grid = persistent_blocks(p.n_vecs, 8, bps);
-  k_alprd<T><<<grid, 256, 0, (cudaStream_t)stream>>>(p);
+  k_alprd<T><<<grid, 256, smem, (cudaStream_t)stream>>>(p);
   note_launch();
   return check_cuda(cudaGetLastError(), "k_alprd launch");
 }
