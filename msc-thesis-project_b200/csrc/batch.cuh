@@ -85,9 +85,9 @@ __global__ void __launch_bounds__(256, batch_min_blocks<T>())
       const size_t vi = v - prefix[c];
       if constexpr (FLOAT) {
         (void)kind;
-        const Meta<T> cur = have_meta ? meta : load_meta<T, XK>(p.c, vi);
+        const Meta<T> cur = have_meta ? meta : load_meta<T, XK>(p.c, vi, t);
         have_meta = v + 1 < end && v + 1 < prefix[c + 1];
-        if (have_meta) meta = load_meta<T, XK>(p.c, vi + 1);
+        if (have_meta) meta = load_meta<T, XK>(p.c, vi + 1, t);
         store_one<T, XK, batch_var<T>()>(p, vi, cur, t);
       } else {
         const Meta<T> cur = have_meta ? meta

@@ -110,7 +110,7 @@ template <typename T> struct Meta {
 };
 
 template <typename T, int KIND>
-__device__ __forceinline__ Meta<T> load_meta(const ColumnParams &c, size_t vi) {
+__device__ __forceinline__ Meta<T> load_meta(const ColumnParams &c, size_t vi, int lane = -1) {
   using U = typename UintOf<T>::U;
   Meta<T> m;
   m.w = c.bw[vi];
@@ -127,6 +127,14 @@ __device__ __forceinline__ Meta<T> load_meta(const ColumnParams &c, size_t vi) {
   if constexpr (KIND == K_ALP) {
     if (c.patch && c.counts) {
       m.ecnt = c.counts[vi];
+      m.eo = c.exc_offs[vi];
+    }
+  } else if constexpr (KIND == K_ALPX) {
+    // ALPExtendedColumn, given the lane: that lane's (count << 10 | offset)
+    // word (the vector's count is their u16 sum, taken at the patch)
+    constexpr int NL = Lanes<typename UintOf<T>::U>::N;
+    if (c.patch && c.oc && lane >= 0) {
+      m.ecnt = lane < NL ? c.oc[vi * NL + lane] : 0u;
       m.eo = c.exc_offs[vi];
     }
   }
@@ -364,9 +372,15 @@ __device__ __forceinline__ void store_one(const KernelParams &p, size_t vi, cons
   // of following the row stores.
   [[maybe_unused]] uint32_t p0 = VEC;
   [[maybe_unused]] T e0 = T(0);
-  [[maybe_unused]] const bool pre = KIND == K_ALP && c.patch && c.counts;
-  if constexpr (KIND == K_ALP) {
-    if (pre && (uint32_t)t < m.ecnt) {
+  [[maybe_unused]] const bool pre =
+      (KIND == K_ALP && c.patch && c.counts) || (KIND == K_ALPX && c.patch && c.oc);
+  [[maybe_unused]] uint32_t ecnt = 0;
+  if constexpr (KIND == K_ALP || KIND == K_ALPX) {
+    if constexpr (KIND == K_ALP)
+      ecnt = m.ecnt;
+    else
+      ecnt = __reduce_add_sync(0xffffffffu, m.ecnt >> 10) & 0xFFFFu;
+    if (pre && (uint32_t)t < ecnt) {
       p0 = c.pos[m.eo + t];
       e0 = reinterpret_cast<const T *>(c.exc)[m.eo + t];
     }
@@ -380,13 +394,13 @@ __device__ __forceinline__ void store_one(const KernelParams &p, size_t vi, cons
       if (idx < lim) store_out<T, decltype(pc)::value>(out + idx, v);
     });
   }
-  if constexpr (KIND == K_ALP) {
+  if constexpr (KIND == K_ALP || KIND == K_ALPX) {
     if (pre) {
       __syncwarp();
-      bool bad = (uint32_t)t < m.ecnt && p0 >= VEC;
+      bool bad = (uint32_t)t < ecnt && p0 >= VEC;
       if ((int)p0 < lim) out[p0] = e0;
       const T *exc = reinterpret_cast<const T *>(c.exc);
-      for (uint32_t i = t + 32; i < m.ecnt; i += 32) {
+      for (uint32_t i = t + 32; i < ecnt; i += 32) {
         const uint32_t ps = c.pos[m.eo + i];
         if (ps < VEC) {
           if ((int)ps < lim) out[ps] = exc[m.eo + i];
@@ -428,9 +442,9 @@ __global__ void __launch_bounds__(256, min_blocks<T, VAR>()) k_store(const Kerne
 
   Meta<T> ma, mb;
   size_t vi = gw;
-  if (vi < n) ma = load_meta<T, KIND>(c, vi);
+  if (vi < n) ma = load_meta<T, KIND>(c, vi, t);
   bool hb = vi + nw < n;
-  if (hb) mb = load_meta<T, KIND>(c, vi + nw);
+  if (hb) mb = load_meta<T, KIND>(c, vi + nw, t);
   while (vi < n) {
     // pair when both vectors are full and share a width marked for pairing
     const bool pair = PM != 0 && hb && ma.w == mb.w && ma.w < 64 && ((PM >> ma.w) & 1) &&
@@ -438,13 +452,13 @@ __global__ void __launch_bounds__(256, min_blocks<T, VAR>()) k_store(const Kerne
     Meta<T> na, nb;
     bool hnb;
     if (pair) {
-      if (vi + 2 * nw < n) na = load_meta<T, KIND>(c, vi + 2 * nw);
+      if (vi + 2 * nw < n) na = load_meta<T, KIND>(c, vi + 2 * nw, t);
       hnb = vi + 3 * nw < n;
-      if (hnb) nb = load_meta<T, KIND>(c, vi + 3 * nw);
+      if (hnb) nb = load_meta<T, KIND>(c, vi + 3 * nw, t);
     } else {
       na = mb;
       hnb = vi + 2 * nw < n;
-      if (hnb) nb = load_meta<T, KIND>(c, vi + 2 * nw);
+      if (hnb) nb = load_meta<T, KIND>(c, vi + 2 * nw, t);
     }
     {
       const size_t vn = vi + (pair ? 2 : 1) * nw;
