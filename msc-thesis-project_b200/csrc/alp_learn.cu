@@ -46,79 +46,91 @@ __device__ __forceinline__ float warp_max_f(float x) {
 // fractions, histograms of the decimal digits after the point (smallest d
 // with x * 10^d integral), of trailing zero bits of the mantissa, of
 // log10|x|, and of the binary exponent.
-// Lane t receives features t and t + 32 (lo, hi); x is the lane's sample.
-__device__ __forceinline__ void vector_features(double x, int t, float &lo_out, float &hi_out) {
-  {
-    const uint64_t bits = (uint64_t)__double_as_longlong(x);
-    const bool fin = isfinite(x);
-    const double a = fabs(x);
-    const bool nz = fin && a > 0.0;
+// Lane t receives features t and t + 32 (lo[r], hi[r]) of R vectors at once
+// (x[r] is the lane's sample of vector r): the R computations are
+// independent straight-line code, so they interleave; each feature is
+// selected into lo / hi as it is computed instead of being held in an
+// array.
+template <int R>
+__device__ __forceinline__ void vector_features(const double (&x)[R], int t, float (&lo)[R],
+                                                float (&hi)[R]) {
+  auto put = [&](int r, int j, float v) {
+    lo[r] = (t == j) ? v : lo[r];
+    hi[r] = (t + 32 == j) ? v : hi[r];
+  };
+#pragma unroll
+  for (int r = 0; r < R; ++r) lo[r] = hi[r] = 0.0f;
+  float l[R];
+  int d[R], tz[R], e2[R];
+  bool fin[R], nz[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const uint64_t bits = (uint64_t)__double_as_longlong(x[r]);
+    fin[r] = isfinite(x[r]);
+    const double a = fabs(x[r]);
+    nz[r] = fin[r] && a > 0.0;
     // log10|x| from the binary exponent and the mantissa in [1, 2) (single
     // precision is far finer than the bf16 features; subnormals in double)
     const int ef = (int)((bits >> 52) & 0x7FF);
     const float mant = __uint_as_float(0x3F800000u | (uint32_t)((bits >> 29) & 0x7FFFFFu));
-    const float l = !nz ? 0.0f
-                        : ef ? __log10f(mant) + (float)(ef - 1023) * 0.30102999566f
-                             : (float)log10(a);
-    int d = 17;
-    if (fin) {
-      for (int dd = 0; dd < 17; ++dd) {
-        const double y = __dmul_rn(x, c_pow10_feat[dd]);
-        if (fabs(y) < 9007199254740992.0 && y == rint(y)) {
-          d = dd;
-          break;
-        }
-      }
+    l[r] = !nz[r] ? 0.0f
+                  : ef ? __log10f(mant) + (float)(ef - 1023) * 0.30102999566f
+                       : (float)log10(a);
+    // decimal digits after the point: the smallest dd < 17 with x * 10^dd
+    // integral (17 when none), without a data-dependent loop exit
+    d[r] = 17;
+#pragma unroll
+    for (int dd = 0; dd < 17; ++dd) {
+      const double y = __dmul_rn(x[r], c_pow10_feat[dd]);
+      if (d[r] == 17 && fin[r] && fabs(y) < 9007199254740992.0 && y == rint(y)) d[r] = dd;
     }
-    int tz = 53;
-    if (nz) {
-      uint64_t mant = bits & 0xFFFFFFFFFFFFFull;
-      if ((bits >> 52) & 0x7FF) mant |= 1ull << 52;
-      tz = __ffsll((long long)mant) - 1;
+    tz[r] = 53;
+    if (nz[r]) {
+      uint64_t mt = bits & 0xFFFFFFFFFFFFFull;
+      if ((bits >> 52) & 0x7FF) mt |= 1ull << 52;
+      tz[r] = __ffsll((long long)mt) - 1;
     }
-    const int e2 = (int)((bits >> 52) & 0x7FF) - 1023;
-    float f[64];
-    const float nnz = (float)__popc(__ballot_sync(0xffffffffu, nz));
+    e2[r] = (int)((bits >> 52) & 0x7FF) - 1023;
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const float nnz = (float)__popc(__ballot_sync(0xffffffffu, nz[r]));
     const float inv = nnz > 0 ? 1.0f / nnz : 0.0f;
-    const float mean_l = warp_sum_f(nz ? l : 0.0f) * inv;
-    const float var_l = warp_sum_f(nz ? (l - mean_l) * (l - mean_l) : 0.0f) * inv;
-    f[0] = mean_l / 10.0f;
-    f[1] = sqrtf(var_l) / 10.0f;
-    f[2] = nnz > 0 ? warp_min_f(nz ? l : 1e30f) / 10.0f : 0.0f;
-    f[3] = nnz > 0 ? warp_max_f(nz ? l : -1e30f) / 10.0f : 0.0f;
-    f[4] = __popc(__ballot_sync(0xffffffffu, fin && a == 0.0)) / 32.0f;
-    f[5] = __popc(__ballot_sync(0xffffffffu, fin && x < 0.0)) / 32.0f;
-    f[6] = __popc(__ballot_sync(0xffffffffu, !fin)) / 32.0f;
+    const float mean_l = warp_sum_f(nz[r] ? l[r] : 0.0f) * inv;
+    const float var_l = warp_sum_f(nz[r] ? (l[r] - mean_l) * (l[r] - mean_l) : 0.0f) * inv;
+    put(r, 0, mean_l / 10.0f);
+    put(r, 1, sqrtf(var_l) / 10.0f);
+    put(r, 2, nnz > 0 ? warp_min_f(nz[r] ? l[r] : 1e30f) / 10.0f : 0.0f);
+    put(r, 3, nnz > 0 ? warp_max_f(nz[r] ? l[r] : -1e30f) / 10.0f : 0.0f);
+    const double a = fabs(x[r]);
+    put(r, 4, __popc(__ballot_sync(0xffffffffu, fin[r] && a == 0.0)) / 32.0f);
+    put(r, 5, __popc(__ballot_sync(0xffffffffu, fin[r] && x[r] < 0.0)) / 32.0f);
+    put(r, 6, __popc(__ballot_sync(0xffffffffu, !fin[r])) / 32.0f);
+    float f7 = 0.0f;
 #pragma unroll
-    for (int b = 0; b < 18; ++b) f[7 + b] = __popc(__ballot_sync(0xffffffffu, d == b)) / 32.0f;
-    const int tzb = tz >= 53 ? 16 : min(15, tz / 4);
-#pragma unroll
-    for (int b = 0; b < 17; ++b) f[25 + b] = __popc(__ballot_sync(0xffffffffu, tzb == b)) / 32.0f;
-    const int lb = nz ? max(0, min(7, (int)floorf((l + 12.0f) / 4.0f))) : -1;
-#pragma unroll
-    for (int b = 0; b < 8; ++b) f[42 + b] = __popc(__ballot_sync(0xffffffffu, lb == b)) / 32.0f;
-    f[50] = warp_sum_f((float)d) / (32.0f * 17.0f);
-    f[51] = warp_max_f((float)d) / 17.0f;
-    f[52] = warp_min_f((float)d) / 17.0f;
-    f[53] = f[7];
-    const float me = warp_sum_f((float)e2) / 32.0f;
-    f[54] = me / 64.0f;
-    f[55] = sqrtf(warp_sum_f(((float)e2 - me) * ((float)e2 - me)) / 32.0f) / 64.0f;
-    f[56] = warp_min_f((float)e2) / 1024.0f;
-    f[57] = warp_max_f((float)e2) / 1024.0f;
-#pragma unroll
-    for (int j = 0; j < 6; ++j)
-      f[58 + j] = __popc(__ballot_sync(0xffffffffu, d <= 2 + 2 * j)) / 32.0f;
-    float lo = 0.0f, hi = 0.0f;
-#pragma unroll
-    for (int j = 0; j < 32; ++j) {
-      if (t == j) {
-        lo = f[j];
-        hi = f[j + 32];
-      }
+    for (int b = 0; b < 18; ++b) {
+      const float v = __popc(__ballot_sync(0xffffffffu, d[r] == b)) / 32.0f;
+      if (b == 0) f7 = v;
+      put(r, 7 + b, v);
     }
-    lo_out = lo;
-    hi_out = hi;
+    const int tzb = tz[r] >= 53 ? 16 : min(15, tz[r] / 4);
+#pragma unroll
+    for (int b = 0; b < 17; ++b) put(r, 25 + b, __popc(__ballot_sync(0xffffffffu, tzb == b)) / 32.0f);
+    const int lb = nz[r] ? max(0, min(7, (int)floorf((l[r] + 12.0f) / 4.0f))) : -1;
+#pragma unroll
+    for (int b = 0; b < 8; ++b) put(r, 42 + b, __popc(__ballot_sync(0xffffffffu, lb == b)) / 32.0f);
+    put(r, 50, warp_sum_f((float)d[r]) / (32.0f * 17.0f));
+    put(r, 51, warp_max_f((float)d[r]) / 17.0f);
+    put(r, 52, warp_min_f((float)d[r]) / 17.0f);
+    put(r, 53, f7);
+    const float me = warp_sum_f((float)e2[r]) / 32.0f;
+    put(r, 54, me / 64.0f);
+    put(r, 55, sqrtf(warp_sum_f(((float)e2[r] - me) * ((float)e2[r] - me)) / 32.0f) / 64.0f);
+    put(r, 56, warp_min_f((float)e2[r]) / 1024.0f);
+    put(r, 57, warp_max_f((float)e2[r]) / 1024.0f);
+#pragma unroll
+    for (int jj = 0; jj < 6; ++jj)
+      put(r, 58 + jj, __popc(__ballot_sync(0xffffffffu, d[r] <= 2 + 2 * jj)) / 32.0f);
   }
 }
 
@@ -127,10 +139,11 @@ __global__ void __launch_bounds__(256) k_features(const double *__restrict__ val
   const int t = threadIdx.x & 31;
   const size_t nw = ((size_t)gridDim.x * blockDim.x) >> 5;
   for (size_t v = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n_vecs; v += nw) {
-    float lo, hi;
-    vector_features(vals[v * VEC + 32 * t], t, lo, hi);
-    feat[v * kFeatures + t] = __float2bfloat16_rn(lo);
-    feat[v * kFeatures + 32 + t] = __float2bfloat16_rn(hi);
+    const double x[1] = {vals[v * VEC + 32 * t]};
+    float lo[1], hi[1];
+    vector_features<1>(x, t, lo, hi);
+    feat[v * kFeatures + t] = __float2bfloat16_rn(lo[0]);
+    feat[v * kFeatures + 32 + t] = __float2bfloat16_rn(hi[0]);
   }
 }
 
@@ -151,20 +164,18 @@ using bf16 = __nv_bfloat16;
 // activations, fp32 logits, ties to the lower class), so the candidates are
 // the same.
 constexpr int kPropRows = 128;
-constexpr int kPropThreads = 512;
+constexpr int kPropThreads = 1024;
+constexpr int kPropGroups = kPropThreads / kPropRows;  // column groups per row
 constexpr int kTopMax = 4;
 constexpr size_t kPropSmem =
     (size_t)(kHidden * kFeatures + kHidden * kHidden + kOut * kHidden + kPropRows * kHidden) * 2 +
-    (size_t)(kHidden + kHidden + kOut) * 4 + (size_t)4 * kPropRows * kTopMax * (4 + 4);
+    (size_t)(kHidden + kHidden + kOut) * 4 + (size_t)kPropGroups * kPropRows * kTopMax * (4 + 4);
 
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
-      "%14,%15}, [%16];\n"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-        "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+                 "=r"(r[6]), "=r"(r[7])
+               : "r"(taddr));
   asm volatile("tcgen05.wait::ld.sync.aligned;");
 }
 
@@ -189,19 +200,21 @@ __device__ __forceinline__ void issue_layer(uint32_t tmem_d, uint32_t sA, uint32
       smem_u32(mbar)));
 }
 
-// Columns [32 q, 32 q + 32) of the row's hidden accumulator at tmem_col +
-// bias, ReLU, to bf16 in the activation tile (K = 128 canonical layout).
+// Columns [HC q, HC q + HC) (HC = 128 / column groups) of the row's hidden
+// accumulator at tmem_col + bias, ReLU, to bf16 in the activation tile
+// (K = 128 canonical layout), 8 columns per tensor-memory load.
 __device__ __forceinline__ void hidden_epilogue(uint32_t tmem, int lanes, int q, int row,
                                                 uint32_t tmem_col, const float *bias,
                                                 unsigned char *sA) {
+  constexpr int HC = kHidden / kPropGroups;
 #pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    const int c0 = 32 * q + 16 * h;
-    uint32_t r[16];
-    tmem_ld16(tmem + ((uint32_t)lanes << 16) + tmem_col + (uint32_t)c0, r);
-    uint32_t packed[8];
+  for (int h = 0; h < HC / 8; ++h) {
+    const int c0 = HC * q + 8 * h;
+    uint32_t r[8];
+    tmem_ld8(tmem + ((uint32_t)lanes << 16) + tmem_col + (uint32_t)c0, r);
+    uint32_t packed[4];
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
+    for (int j = 0; j < 4; ++j) {
       const float a = fmaxf(__uint_as_float(r[2 * j]) + bias[c0 + 2 * j], 0.0f);
       const float b = fmaxf(__uint_as_float(r[2 * j + 1]) + bias[c0 + 2 * j + 1], 0.0f);
       const __nv_bfloat162 hv = __floats2bfloat162_rn(a, b);
@@ -209,8 +222,6 @@ __device__ __forceinline__ void hidden_epilogue(uint32_t tmem, int lanes, int q,
     }
     *reinterpret_cast<uint4 *>(sA + canon_off(row, c0, kPropRows)) =
         make_uint4(packed[0], packed[1], packed[2], packed[3]);
-    *reinterpret_cast<uint4 *>(sA + canon_off(row, c0 + 8, kPropRows)) =
-        make_uint4(packed[4], packed[5], packed[6], packed[7]);
   }
 }
 
@@ -246,10 +257,10 @@ __global__ void __launch_bounds__(kPropThreads, 1)
   float *sb1 = reinterpret_cast<float *>(sA + kPropRows * kHidden * 2);
   float *sb2 = sb1 + kHidden;
   float *sb3 = sb2 + kHidden;
-  float *s_topv = sb3 + kOut;                                         // [4][128][kTopMax]
-  int *s_topc = reinterpret_cast<int *>(s_topv + 4 * kPropRows * kTopMax);
+  float *s_topv = sb3 + kOut;  // [column groups][128][kTopMax]
+  int *s_topc = reinterpret_cast<int *>(s_topv + kPropGroups * kPropRows * kTopMax);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int lanes = 32 * (warp & 3), quarter = warp >> 2, row = lanes + lane;
+  const int lanes = 32 * (warp & 3), quarter = warp >> 2, row = lanes + lane;  // quarter: column group
   constexpr uint32_t kCols = 256;
 
   // weights and biases, once per CTA
@@ -288,7 +299,7 @@ __global__ void __launch_bounds__(kPropThreads, 1)
   uint32_t phase = 0;
   bool failed = false;
   const size_t n_tiles = (n_vecs + kPropRows - 1) / kPropRows;
-  constexpr int kRowsPerWarp = kPropRows / (kPropThreads / 32);  // 8
+  constexpr int kRowsPerWarp = kPropRows / (kPropThreads / 32);
 
   for (size_t tile = blockIdx.x; tile < n_tiles && !failed; tile += gridDim.x) {
     const size_t m0 = tile * kPropRows;
@@ -301,12 +312,17 @@ __global__ void __launch_bounds__(kPropThreads, 1)
       xs[i] = v < n_vecs ? vals[v * VEC + 32 * lane] : 0.0;
     }
 #pragma unroll
-    for (int i = 0; i < kRowsPerWarp; ++i) {
-      float lo, hi;
-      vector_features(xs[i], lane, lo, hi);
-      const int r = warp * kRowsPerWarp + i;
-      *reinterpret_cast<bf16 *>(sA + canon_off(r, lane, kPropRows)) = __float2bfloat16_rn(lo);
-      *reinterpret_cast<bf16 *>(sA + canon_off(r, lane + 32, kPropRows)) = __float2bfloat16_rn(hi);
+    for (int i = 0; i < kRowsPerWarp; i += 2) {
+      const double x2[2] = {xs[i], xs[i + 1]};
+      float lo[2], hi[2];
+      vector_features<2>(x2, lane, lo, hi);
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const int r = warp * kRowsPerWarp + i + q;
+        *reinterpret_cast<bf16 *>(sA + canon_off(r, lane, kPropRows)) = __float2bfloat16_rn(lo[q]);
+        *reinterpret_cast<bf16 *>(sA + canon_off(r, lane + 32, kPropRows)) =
+            __float2bfloat16_rn(hi[q]);
+      }
     }
     asm volatile("fence.proxy.async.shared::cta;");
     asm volatile("tcgen05.fence::before_thread_sync;");
@@ -343,9 +359,10 @@ __global__ void __launch_bounds__(kPropThreads, 1)
     }
     phase ^= 1u;
     asm volatile("tcgen05.fence::after_thread_sync;");
-    // top-k of this quarter of the row's logits (classes 48 q .. 48 q + 47;
-    // class 191 is padding)
+    // top-k of this group's share of the row's logits (LC classes from
+    // LC q; class 191 is padding)
     {
+      constexpr int LC = kOut / kPropGroups;
       float bv[kTopMax];
       int bc[kTopMax];
 #pragma unroll
@@ -354,12 +371,12 @@ __global__ void __launch_bounds__(kPropThreads, 1)
         bc[q] = -1;
       }
 #pragma unroll
-      for (int h = 0; h < 3; ++h) {
-        const int c0 = 48 * quarter + 16 * h;
-        uint32_t r[16];
-        tmem_ld16(tmem + ((uint32_t)lanes << 16) + (uint32_t)c0, r);
+      for (int h = 0; h < LC / 8; ++h) {
+        const int c0 = LC * quarter + 8 * h;
+        uint32_t r[8];
+        tmem_ld8(tmem + ((uint32_t)lanes << 16) + (uint32_t)c0, r);
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
+        for (int j = 0; j < 8; ++j) {
           const int c = c0 + j;
           if (c < kClasses) top_insert(bv, bc, k, __uint_as_float(r[j]) + sb3[c], c);
         }
@@ -382,7 +399,7 @@ __global__ void __launch_bounds__(kPropThreads, 1)
         bv[q] = s_topv[row * kTopMax + q];
         bc[q] = s_topc[row * kTopMax + q];
       }
-      for (int qq = 1; qq < 4; ++qq)
+      for (int qq = 1; qq < kPropGroups; ++qq)
 #pragma unroll
         for (int q = 0; q < kTopMax; ++q)
           top_insert(bv, bc, k, s_topv[(qq * kPropRows + row) * kTopMax + q],
