@@ -472,12 +472,23 @@ __global__ void k_relu_back(const float *__restrict__ dxf, const __nv_bfloat16 *
 }
 
 // db[c] = sum over rows of g[r][c] (g bf16), one thread per column
-__global__ void k_colsum_bf16(const __nv_bfloat16 *__restrict__ g, int rows, int cols, float *db) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= cols) return;
+// Column sums (bias gradients): a block of 32 x 32 threads per 32 columns;
+// thread (c, y) adds rows y, y + 32, ... of column c, then the 32 partial
+// sums of a column are added in shared memory.
+__global__ void __launch_bounds__(1024) k_colsum_bf16(const __nv_bfloat16 *__restrict__ g,
+                                                      int rows, int cols, float *db) {
+  __shared__ float part[32][33];
+  const int c = blockIdx.x * 32 + threadIdx.x, y = threadIdx.y;
   float s = 0.0f;
-  for (int r = 0; r < rows; ++r) s += __bfloat162float(g[(size_t)r * cols + c]);
-  db[c] = s;
+  if (c < cols)
+    for (int r = y; r < rows; r += 32) s += __bfloat162float(g[(size_t)r * cols + c]);
+  part[y][threadIdx.x] = s;
+  __syncthreads();
+  if (y == 0 && c < cols) {
+    float t = 0.0f;
+    for (int i = 0; i < 32; ++i) t += part[i][threadIdx.x];
+    db[c] = t;
+  }
 }
 
 // Adam on fp32 master parameters; refreshes the bf16 copy (and its
@@ -726,7 +737,7 @@ flsgpu_status forward_backward(flsgpu_alp_encoder *e, const bf16 *x, const int16
   if ((st = gemm_tn(gemm(e->t_a, rows, e->t_b, rows, kOut, kHidden, rows, e->g + kOffW3, nullptr,
                          kHidden, nullptr, 0, e->status), s)))
     return st;
-  k_colsum_bf16<<<1, kOut, 0, s>>>(e->dz, rows, kOut, e->g + kOffB3);
+  k_colsum_bf16<<<(kOut + 31) / 32, dim3(32, 32), 0, s>>>(e->dz, rows, kOut, e->g + kOffB3);
   if ((st = gemm_tn(gemm(e->dz, kOut, e->w3t, kOut, rows, kHidden, kOut, e->tmpf, nullptr, kHidden,
                          nullptr, 0, e->status), s)))
     return st;
@@ -737,7 +748,7 @@ flsgpu_status forward_backward(flsgpu_alp_encoder *e, const bf16 *x, const int16
   if ((st = gemm_tn(gemm(e->t_a, rows, e->t_b, rows, kHidden, kHidden, rows, e->g + kOffW2, nullptr,
                          kHidden, nullptr, 0, e->status), s)))
     return st;
-  k_colsum_bf16<<<1, kHidden, 0, s>>>(e->dh, rows, kHidden, e->g + kOffB2);
+  k_colsum_bf16<<<(kHidden + 31) / 32, dim3(32, 32), 0, s>>>(e->dh, rows, kHidden, e->g + kOffB2);
   if ((st = gemm_tn(gemm(e->dh, kHidden, e->w2t, kHidden, rows, kHidden, kHidden, e->tmpf, nullptr,
                          kHidden, nullptr, 0, e->status), s)))
     return st;
@@ -748,7 +759,7 @@ flsgpu_status forward_backward(flsgpu_alp_encoder *e, const bf16 *x, const int16
   if ((st = gemm_tn(gemm(e->t_a, rows, e->t_b, rows, kHidden, kFeatures, rows, e->g + kOffW1,
                          nullptr, kFeatures, nullptr, 0, e->status), s)))
     return st;
-  k_colsum_bf16<<<1, kHidden, 0, s>>>(e->dh, rows, kHidden, e->g + kOffB1);
+  k_colsum_bf16<<<(kHidden + 31) / 32, dim3(32, 32), 0, s>>>(e->dh, rows, kHidden, e->g + kOffB1);
   note_launch(5);
   return check_cuda(cudaGetLastError(), "backward");
 }
