@@ -225,6 +225,7 @@ __device__ __forceinline__ int64_t enc_checked(double x, int f, int e, bool *is_
 }
 
 struct VecAnalysis {
+  uint32_t mask;  // this thread's exceptions (bit k: value k of its 32)
   int n_exc;
   int bw;
   int64_t fill;   // the integer stored at exception positions
@@ -255,6 +256,7 @@ __device__ VecAnalysis analyze_vector(const double *__restrict__ vec, int e, int
 #pragma unroll
   for (int s = 16; s >= 1; s >>= 1) first_ok = min(first_ok, __shfl_xor_sync(0xffffffffu, first_ok, s));
   VecAnalysis a;
+  a.mask = exc_mask;
   a.n_exc = __reduce_add_sync(0xffffffffu, __popc(exc_mask));
   // the first non-exception's integer (0 when every position, or every
   // position but the last, is an exception: encoder.hpp:361-367)
@@ -274,24 +276,25 @@ __device__ VecAnalysis analyze_vector(const double *__restrict__ vec, int e, int
 
 // Packed words (bw * 16 u64 at `packed`) and exceptions (value, position,
 // ascending position) at `exc` / `pos` of one vector, staged in the warp's
-// shared copy `sv` of the vector (filled and synchronised by the caller).
+// shared copy `sv` of the vector (filled and synchronised by the caller);
+// exc_mask is this thread's exception mask from the analysis, so only the
+// non-exceptions are encoded here (no decode, no comparison).
 __device__ void pack_vector(const double *sv, int e, int f, int t, int64_t fill, uint64_t base,
-                            int bw, uint64_t *packed, double *exc, uint16_t *pos) {
+                            int bw, uint32_t exc_mask, uint64_t *packed, double *exc,
+                            uint16_t *pos) {
   const int lane = t & 15, half = t >> 4;
-  uint32_t exc_mask = 0;
   // this thread's 32 values are bits [32*half*bw, 32*(half+1)*bw) of the
   // lane stream = its bw 32-bit words, owned by it alone
   uint32_t *p32 = reinterpret_cast<uint32_t *>(packed) + 2 * lane;
   const uint64_t mask = bw >= 64 ? ~0ull : ((1ull << bw) - 1);
   uint32_t acc = 0;  // pending low bits (< 32 of them)
   int nacc = 0, m = half * bw;
+  if (bw > 0) {
 #pragma unroll 2
-  for (int k = 0; k < 32; ++k) {
-    bool is_exc;
-    int64_t q = enc_checked(sv[lane + 16 * (32 * half + k)], f, e, &is_exc);
-    exc_mask |= (uint32_t)is_exc << k;
-    if (is_exc) q = fill;
-    if (bw > 0) {
+    for (int k = 0; k < 32; ++k) {
+      const int64_t q = ((exc_mask >> k) & 1)
+                            ? fill
+                            : enc_value(sv[lane + 16 * (32 * half + k)], f, e, false);
       const uint64_t d = ((uint64_t)q - base) & mask;
       // (hi:lo) = acc | d << nacc, total = nacc + bw bits (at most 95)
       uint64_t lo = (uint64_t)acc | (d << nacc);
@@ -401,6 +404,7 @@ __global__ void __launch_bounds__(256)
       }
       continue;
     }
+    sl.exc_mask[v * 32 + t] = a.mask;
     if (t == 0) {
       sl.bw[v] = (uint8_t)a.bw;
       sl.base[v] = a.base;
@@ -432,6 +436,7 @@ __global__ void __launch_bounds__(256)
     plain_search(smp, t, nullptr, &pair);
     const int e = class_exp(pair), f = class_fac(pair);
     const VecAnalysis a = analyze_vector(vec, e, f, t);
+    sl.exc_mask[v * 32 + t] = a.mask;
     if (t == 0) {
       sl.bw[v] = (uint8_t)a.bw;
       sl.base[v] = a.base;
@@ -575,8 +580,8 @@ __global__ void __launch_bounds__(256) k_alp_pack(const double *__restrict__ val
       off_words[v] = ow;  // the column's final offsets
       off_exc[v] = oe;
     }
-    pack_vector(sv, sl.exp[v], sl.fac[v], t, sl.fill[v], sl.base[v], sl.bw[v], packed + ow,
-                exc + oe, pos + oe);
+    pack_vector(sv, sl.exp[v], sl.fac[v], t, sl.fill[v], sl.base[v], sl.bw[v],
+                sl.exc_mask[v * 32 + t], packed + ow, exc + oe, pos + oe);
   }
 }
 

@@ -645,7 +645,7 @@ flsgpu_status ensure_rows(flsgpu_alp_encoder *e, int rows) {
 void free_enc(flsgpu_alp_encoder *e) {
   for (void *p : {(void *)e->feat, (void *)e->labels, (void *)e->cand, (void *)e->sl.fill,
                   (void *)e->sl.fb_list, (void *)e->sl.fb_count, (void *)e->sl.blk_words,
-                  (void *)e->sl.blk_exc,
+                  (void *)e->sl.blk_exc, (void *)e->sl.exc_mask,
                   (void *)e->sl.bw, (void *)e->sl.base,
                   (void *)e->sl.fac, (void *)e->sl.exp, (void *)e->sl.count, (void *)e->sl.flags,
                   (void *)e->off_words, (void *)e->off_exc, (void *)e->totals, (void *)e->packed,
@@ -674,6 +674,7 @@ flsgpu_status ensure_vecs(flsgpu_alp_encoder *e, size_t n_vecs) {
   e->sl.fb_count = dalloc<uint32_t>(1, st);
   e->sl.blk_words = dalloc<size_t>(n / 1024 + 1, st);
   e->sl.blk_exc = dalloc<size_t>(n / 1024 + 1, st);
+  e->sl.exc_mask = dalloc<uint32_t>(n * 32, st);
   e->sl.bw = dalloc<uint8_t>(n, st);
   e->sl.base = dalloc<uint64_t>(n, st);
   e->sl.fac = dalloc<uint8_t>(n, st);

@@ -43,6 +43,7 @@ struct EncodeSlots {
   uint32_t *fb_count;
   size_t *blk_words;  // per 1024 vectors: offsets of the scan's blocks
   size_t *blk_exc;
+  uint32_t *exc_mask; // per vector, 32 words: thread t's exception bits
 };
 
 // Launchers (alp_encode.cu)
