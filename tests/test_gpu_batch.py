@@ -132,3 +132,40 @@ def test_pair_query_median_and_masked_sum(cuda, graph):
         assert meds[i] == med, f"pair {i}"
         assert res[i].view(np.uint64) == np.float64(want).view(np.uint64), f"pair {i}"
     assert int(q.status.item()) == 0
+
+
+def test_pair_query_ragged_lengths(cuda):
+    """Columns whose length is not a multiple of 1024: the median and the
+    masked sum cover only the valid values (the oracle sees the last vector
+    padded with B = 0xFFFFFFFF, which is never below the median, and with the
+    median taken over the n valid values)."""
+    import torch
+    o = B.oracle()
+    pairs, wants = [], []
+    for i, n_values in enumerate((1000, 5 * 1024 + 17, 3 * 1024 - 1)):
+        n_vecs = (n_values + 1023) // 1024
+        col_a = colgen.random_alp(300 + i, n_vecs, True, range(8, 22), range(0, 20))
+        e = col_a["exceptions"]
+        col_a["exceptions"] = np.where(np.isfinite(e), e, 0.75)
+        cb = colgen.random_ffor(310 + i, n_vecs, 32, range(0, 33), n_values=n_values)
+        a = F.make_alp_column(col_a, n_values, np.float64, device=cuda)
+        b = F.make_ffor_column(cb["packed"], cb["bit_widths"], cb["vector_offsets"], cb["bases"],
+                               n_values, cuda)
+        av = B.alp_decode(col_a, n_vecs, np.float64)
+        bv = B.decode_ffor(cb["packed"], cb["bit_widths"], cb["vector_offsets"], cb["bases"], 32)
+        bv = np.ascontiguousarray(bv.astype(np.uint32))
+        med = int(o.orc_median_u32(B.ptr(bv), n_values))
+        bpad = bv.copy()
+        bpad[n_values:] = 0xFFFFFFFF
+        want = o.orc_tree_sum_masked_f64(B.ptr(av), B.ptr(bpad), med, n_vecs)
+        pairs.append((a, b))
+        wants.append((med, want))
+    q = F.PairQuery([p[0] for p in pairs], [p[1] for p in pairs], cuda)
+    q.run()
+    torch.cuda.synchronize()
+    meds = q.medians.cpu().numpy().view(np.uint32)
+    res = q.results.cpu().numpy()
+    for i, (med, want) in enumerate(wants):
+        assert meds[i] == med, i
+        assert res[i].view(np.uint64) == np.float64(want).view(np.uint64), i
+    assert int(q.status.item()) == 0

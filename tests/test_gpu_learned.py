@@ -191,3 +191,43 @@ def test_fused_proposal_matches_layered(cuda):
         fused = enc.propose(vals, k)
         layered = enc.propose(vals, k, layered=True)
         assert torch.equal(fused, layered), k
+
+
+def test_encoder_edge_vectors(cuda):
+    """Vectors at the ends of the encoder's rules, each checked against the
+    oracle encoder and decoded exactly: every value an exception (NaN),
+    every value but the last an exception (the fill integer is then 0),
+    a constant vector (width 0), and a vector of one repeated decimal with
+    a single exception."""
+    import torch
+    rng = np.random.default_rng(5)
+    vecs = [np.full(1024, np.nan),
+            np.concatenate([np.full(1023, np.inf), [7.0]]),
+            np.full(1024, 3.25),
+            np.where(np.arange(1024) == 700, np.pi, 12.5),
+            np.round(rng.uniform(-1000, 1000, 1024), 2)]
+    vals = np.concatenate(vecs).astype(np.float64)
+    n_vecs = len(vecs)
+    enc = F.AlpEncoder(seed=2)
+    res = enc.encode(torch.from_numpy(vals).to(cuda), 0)
+    col = F.encoded_column(res, vals.size, enc)
+    got = F.decompress(col).cpu().numpy().view(np.uint64)
+    assert np.array_equal(got, vals.view(np.uint64))
+    c = res.column
+    host = lambda ptr, n, dt: F.device_array(ptr, n, dt).cpu().numpy()  # noqa: E731
+    counts = host(c.counts, n_vecs, np.uint16)
+    bw = host(c.ffor.bp.bit_widths, n_vecs, np.uint8)
+    fac = host(c.factor_indices, n_vecs, np.uint8)
+    exp = host(c.fraction_indices, n_vecs, np.uint8)
+    o = B.oracle()
+    for i in range(n_vecs):
+        vec = np.ascontiguousarray(vals[i * 1024:(i + 1) * 1024])
+        ints = np.zeros(1024, np.int64)
+        ex = np.zeros(1024, np.float64)
+        ps = np.zeros(1024, np.uint16)
+        n_exc = o.orc_alp_encode_vector_f64(B.ptr(vec), int(exp[i]), int(fac[i]), B.ptr(ints),
+                                            B.ptr(ex), B.ptr(ps))
+        assert n_exc == counts[i], i
+        mn = int(ints.min())
+        assert int(int(ints.max()) - mn).bit_length() == bw[i], i
+    assert counts[0] == 1024 and counts[1] == 1023 and bw[2] == 0 and counts[3] == 1
