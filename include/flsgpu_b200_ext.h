@@ -101,6 +101,27 @@ flsgpu_status flsgpu_host_decompress_alp_f32(flsgpu_host_pipeline *pipeline,
 flsgpu_status flsgpu_host_decompress_alp_f64(flsgpu_host_pipeline *pipeline,
                                              const flsgpu_alp_column *host_column,
                                              double *host_out, const flsgpu_decode_opts *opts);
+/* The same without waiting: the chunks join the pipeline's queue behind
+ * those of earlier calls (the slots alternate across calls), so a series of
+ * columns streams without draining between them.  The host arrays and
+ * host_out of every call must stay valid and untouched until
+ * flsgpu_host_pipeline_sync returns; the outputs are complete only then.
+ * Columns must use the built-in factor / fraction tables. */
+flsgpu_status flsgpu_host_decompress_ffor_u32_async(flsgpu_host_pipeline *pipeline,
+                                                    const flsgpu_ffor_column *host_column,
+                                                    uint32_t *host_out,
+                                                    const flsgpu_decode_opts *opts);
+flsgpu_status flsgpu_host_decompress_ffor_u64_async(flsgpu_host_pipeline *pipeline,
+                                                    const flsgpu_ffor_column *host_column,
+                                                    uint64_t *host_out,
+                                                    const flsgpu_decode_opts *opts);
+flsgpu_status flsgpu_host_decompress_alp_f32_async(flsgpu_host_pipeline *pipeline,
+                                                   const flsgpu_alp_column *host_column,
+                                                   float *host_out, const flsgpu_decode_opts *opts);
+flsgpu_status flsgpu_host_decompress_alp_f64_async(flsgpu_host_pipeline *pipeline,
+                                                   const flsgpu_alp_column *host_column,
+                                                   double *host_out, const flsgpu_decode_opts *opts);
+flsgpu_status flsgpu_host_pipeline_sync(flsgpu_host_pipeline *pipeline);
 
 /* ---- fused pair query over compressed columns (no reference counterpart)
  * For each pair i: d_results[i] = sum of A_i[k] over positions k with

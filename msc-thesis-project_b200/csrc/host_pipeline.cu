@@ -22,6 +22,7 @@
 
 struct flsgpu_host_pipeline {
   size_t chunk_vecs = 0;
+  size_t seq = 0;  // chunks issued so far: slots alternate across calls
   cudaStream_t in = nullptr, comp = nullptr, out = nullptr;
   cudaEvent_t ev_in[2] = {}, ev_comp[2] = {}, ev_out[2] = {};
   // per slot: packed words, per-vector metadata, exceptions, output
@@ -120,11 +121,11 @@ static flsgpu_status stage_alp(flsgpu_host_pipeline *p, int sl, const flsgpu_alp
 // (output) of the chunk two before.
 template <typename T, typename Col, typename Stage, typename Decode>
 static flsgpu_status run_pipeline(flsgpu_host_pipeline *p, const Col *hc, size_t n_values,
-                                  T *host_out, Stage &&stage, Decode &&decode) {
+                                  T *host_out, bool wait, Stage &&stage, Decode &&decode) {
   const size_t n_vecs = (n_values + 1023) / 1024;
   flsgpu_status st = FLSGPU_OK;
-  for (size_t c = 0, v0 = 0; v0 < n_vecs && !st; ++c, v0 += p->chunk_vecs) {
-    const int sl = (int)(c & 1);
+  for (size_t v0 = 0; v0 < n_vecs && !st; v0 += p->chunk_vecs) {
+    const int sl = (int)(p->seq++ & 1);
     const size_t v1 = v0 + p->chunk_vecs < n_vecs ? v0 + p->chunk_vecs : n_vecs;
     if ((st = check_cuda(cudaStreamWaitEvent(p->in, p->ev_comp[sl], 0), "wait"))) break;
     Col dc;
@@ -144,6 +145,7 @@ static flsgpu_status run_pipeline(flsgpu_host_pipeline *p, const Col *hc, size_t
         (st = check_cuda(cudaEventRecord(p->ev_out[sl], p->out), "record")))
       break;
   }
+  if (!wait && !st) return FLSGPU_OK;
   flsgpu_status ss = check_cuda(cudaStreamSynchronize(p->out), "sync");
   cudaStreamSynchronize(p->comp);
   cudaStreamSynchronize(p->in);
@@ -154,12 +156,12 @@ static flsgpu_status run_pipeline(flsgpu_host_pipeline *p, const Col *hc, size_t
 // descriptor's per-vector arrays so that index v0.. maps to 0..
 template <typename T>
 static flsgpu_status host_ffor(flsgpu_host_pipeline *p, const flsgpu_ffor_column *hc, T *host_out,
-                               const flsgpu_decode_opts *o) {
+                               const flsgpu_decode_opts *o, bool wait) {
   if (!p || !hc || !host_out) return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "null argument");
   if (!hc->bp.bit_widths || !hc->bp.vector_offsets || !hc->bp.packed_array)
     return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "null host array");
   return run_pipeline<T>(
-      p, hc, hc->n_values, host_out,
+      p, hc, hc->n_values, host_out, wait,
       [&](int sl, size_t v0, size_t v1, flsgpu_ffor_column &dc) {
         return stage_ffor<T>(p, sl, hc, v0, v1, dc);
       },
@@ -173,13 +175,16 @@ static flsgpu_status host_ffor(flsgpu_host_pipeline *p, const flsgpu_ffor_column
 
 template <typename T>
 static flsgpu_status host_alp(flsgpu_host_pipeline *p, const flsgpu_alp_column *hc, T *host_out,
-                              const flsgpu_decode_opts *o) {
+                              const flsgpu_decode_opts *o, bool wait) {
   if (!p || !hc || !host_out) return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "null argument");
   if (!hc->ffor.bp.bit_widths || !hc->ffor.bp.vector_offsets || !hc->ffor.bp.packed_array ||
       !hc->ffor.bases || !hc->factor_indices || !hc->fraction_indices ||
       !hc->exceptions_offsets || !hc->counts)
     return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "null host array");
   constexpr bool F64 = sizeof(T) == 8;
+  if (!wait && (hc->factors || hc->fractions))
+    return set_error(FLSGPU_ERR_UNSUPPORTED,
+                     "asynchronous host decode needs the built-in factor / fraction tables");
   if (hc->factors || hc->fractions) {
     flsgpu_status st = FLSGPU_OK;
     if (hc->factors)
@@ -192,7 +197,7 @@ static flsgpu_status host_alp(flsgpu_host_pipeline *p, const flsgpu_alp_column *
     if (st) return st;
   }
   return run_pipeline<T>(
-      p, hc, hc->n_values, host_out,
+      p, hc, hc->n_values, host_out, wait,
       [&](int sl, size_t v0, size_t v1, flsgpu_alp_column &dc) {
         return stage_alp<T>(p, sl, hc, v0, v1, dc);
       },
@@ -261,19 +266,46 @@ flsgpu_status flsgpu_host_pipeline_create(size_t chunk_values, flsgpu_host_pipel
 
 flsgpu_status flsgpu_host_decompress_ffor_u32(flsgpu_host_pipeline *p, const flsgpu_ffor_column *c,
                                               uint32_t *host_out, const flsgpu_decode_opts *o) {
-  return host_ffor<uint32_t>(p, c, host_out, o);
+  return host_ffor<uint32_t>(p, c, host_out, o, true);
 }
 flsgpu_status flsgpu_host_decompress_ffor_u64(flsgpu_host_pipeline *p, const flsgpu_ffor_column *c,
                                               uint64_t *host_out, const flsgpu_decode_opts *o) {
-  return host_ffor<uint64_t>(p, c, host_out, o);
+  return host_ffor<uint64_t>(p, c, host_out, o, true);
 }
 flsgpu_status flsgpu_host_decompress_alp_f32(flsgpu_host_pipeline *p, const flsgpu_alp_column *c,
                                              float *host_out, const flsgpu_decode_opts *o) {
-  return host_alp<float>(p, c, host_out, o);
+  return host_alp<float>(p, c, host_out, o, true);
 }
 flsgpu_status flsgpu_host_decompress_alp_f64(flsgpu_host_pipeline *p, const flsgpu_alp_column *c,
                                              double *host_out, const flsgpu_decode_opts *o) {
-  return host_alp<double>(p, c, host_out, o);
+  return host_alp<double>(p, c, host_out, o, true);
+}
+flsgpu_status flsgpu_host_decompress_ffor_u32_async(flsgpu_host_pipeline *p,
+                                                    const flsgpu_ffor_column *c, uint32_t *host_out,
+                                                    const flsgpu_decode_opts *o) {
+  return host_ffor<uint32_t>(p, c, host_out, o, false);
+}
+flsgpu_status flsgpu_host_decompress_ffor_u64_async(flsgpu_host_pipeline *p,
+                                                    const flsgpu_ffor_column *c, uint64_t *host_out,
+                                                    const flsgpu_decode_opts *o) {
+  return host_ffor<uint64_t>(p, c, host_out, o, false);
+}
+flsgpu_status flsgpu_host_decompress_alp_f32_async(flsgpu_host_pipeline *p,
+                                                   const flsgpu_alp_column *c, float *host_out,
+                                                   const flsgpu_decode_opts *o) {
+  return host_alp<float>(p, c, host_out, o, false);
+}
+flsgpu_status flsgpu_host_decompress_alp_f64_async(flsgpu_host_pipeline *p,
+                                                   const flsgpu_alp_column *c, double *host_out,
+                                                   const flsgpu_decode_opts *o) {
+  return host_alp<double>(p, c, host_out, o, false);
+}
+flsgpu_status flsgpu_host_pipeline_sync(flsgpu_host_pipeline *p) {
+  if (!p) return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "null pipeline");
+  flsgpu_status st = check_cuda(cudaStreamSynchronize(p->out), "sync");
+  cudaStreamSynchronize(p->comp);
+  cudaStreamSynchronize(p->in);
+  return st;
 }
 
 }  // extern "C"

@@ -391,10 +391,17 @@ class HostPipeline:
         self.h = P()
         _check(_fn("flsgpu_host_pipeline_create")(SZ(chunk_values), C.byref(self.h)))
 
-    def decompress(self, desc, kind: str, dtype: str, host_out, o: DecodeOpts | None = None):
-        _check(_fn(f"flsgpu_host_decompress_{kind}_{dtype}")(
-            self.h, C.byref(desc), P(host_out.data_ptr()), C.byref(o) if o is not None else None))
+    def decompress(self, desc, kind: str, dtype: str, host_out, o: DecodeOpts | None = None,
+                   wait: bool = True):
+        """wait=False queues the column behind earlier ones (sync() waits);
+        its host arrays must stay alive and untouched until then."""
+        name = f"flsgpu_host_decompress_{kind}_{dtype}" + ("" if wait else "_async")
+        _check(_fn(name)(self.h, C.byref(desc), P(host_out.data_ptr()),
+                         C.byref(o) if o is not None else None))
         return host_out
+
+    def sync(self):
+        _check(_fn("flsgpu_host_pipeline_sync")(self.h))
 
     def __del__(self):
         if getattr(self, "h", None):

@@ -60,3 +60,26 @@ def test_host_pipeline_alp(cuda, f64):
     pipe.decompress(c, "alp", "f64" if f64 else "f32", out)
     want = B.alp_decode(col, n_vecs, dt).view(ut)
     assert np.array_equal(out.numpy().view(ut), want)
+
+
+def test_host_pipeline_async_series(cuda):
+    """Several columns queued without waiting, then one sync: every output
+    matches the oracle."""
+    import torch
+    pipe = F.HostPipeline(chunk_values=2048)
+    jobs = []
+    for i, (bits, n_values) in enumerate([(32, 5 * 1024 + 3), (64, 3 * 1024), (32, 2048)]):
+        n_vecs = (n_values + 1023) // 1024
+        c = colgen.random_ffor(70 + i, n_vecs, bits, range(bits + 1), n_values=n_values)
+        sd = np.int64 if bits == 64 else np.int32
+        t = [_pinned(c["packed"].view(sd)), _pinned(c["bit_widths"]),
+             _pinned(c["vector_offsets"].view(np.int64)), _pinned(c["bases"].view(sd))]
+        desc, kind, dt, keep = F.host_ffor_column(*t, n_values)
+        out = torch.empty(n_values, dtype=torch.int64 if bits == 64 else torch.int32).pin_memory()
+        pipe.decompress(desc, kind, dt, out, wait=False)
+        jobs.append((c, bits, n_values, out, keep, desc))
+    pipe.sync()
+    for c, bits, n_values, out, *_ in jobs:
+        ut = np.uint64 if bits == 64 else np.uint32
+        want = B.decode_ffor(c["packed"], c["bit_widths"], c["vector_offsets"], c["bases"], bits)
+        assert np.array_equal(out.numpy().view(ut), want[:n_values])
