@@ -392,6 +392,72 @@ def make_alp_columns(scale: float, dev, seed: int = 31):
     return out
 
 
+def cpu_reference_alp(cols, seconds_budget: float = 5.0, sample_vecs: int = 16384):
+    """The reference's own CPU ALP decoder (alp::decode: falp + patch
+    exceptions, compiled from the reference sources into oracle/_ref) on all
+    host threads, over the first sample_vecs vectors of the f64 and f32 ALP
+    columns (copied to host memory).  None when oracle/_ref is absent."""
+    import flsgpu_b200 as F
+    from oracle import binding as B
+    r = B.ref()
+    if r is None:
+        return None
+    threads = os.cpu_count() or 1
+    work, bytes_one = [], 0
+    for name, col, vals, rb, wb in cols:
+        if name not in ("alp_f64", "alp_f32"):
+            continue
+        f64 = name == "alp_f64"
+        ut, ft = (np.uint64, np.float64) if f64 else (np.uint32, np.float32)
+        nl = 16 if f64 else 32
+        c = col.c
+        nv = min(sample_vecs, col.n_vecs)
+        h = lambda ptr, n, dt: F.device_array(ptr, n, dt).cpu().numpy().view(dt)  # noqa: E731
+        bw = h(c.ffor.bp.bit_widths, nv, np.uint8)
+        offs = h(c.ffor.bp.vector_offsets, nv, np.uint64)
+        counts = h(c.counts, nv, np.uint16)
+        eoffs = h(c.exceptions_offsets, nv, np.uint64)
+        n_words = int(offs[-1]) + int(bw[-1]) * nl
+        n_exc = int(eoffs[-1]) + int(counts[-1])
+        arrs = dict(packed=h(c.ffor.bp.packed_array, max(n_words, 1), ut), bw=bw, offs=offs,
+                    bases=h(c.ffor.bases, nv, ut), fac=h(c.factor_indices, nv, np.uint8),
+                    exp=h(c.fraction_indices, nv, np.uint8), eoffs=eoffs,
+                    exc=h(c.exceptions, max(n_exc, 1), ft), pos=h(c.positions, max(n_exc, 1), np.uint16),
+                    counts=counts, out=np.zeros(nv * 1024, ft))
+        work.append((f64, nv, arrs))
+        bytes_one += n_words * (8 if f64 else 4) + nv * (29 if f64 else 25) + n_exc * (10 if f64 else 6) \
+            + nv * 1024 * (8 if f64 else 4)
+
+    def run_one(f64, a, v0, v1):
+        fn = r.ref_decode_alp_f64 if f64 else r.ref_decode_alp_f32
+        fn(B.ptr(a["packed"]), B.ptr(a["bw"]), B.ptr(a["offs"]), B.ptr(a["bases"]), B.ptr(a["fac"]),
+           B.ptr(a["exp"]), B.ptr(a["eoffs"]), B.ptr(a["exc"]), B.ptr(a["pos"]), B.ptr(a["counts"]),
+           v0, v1, B.ptr(a["out"]))
+
+    def one_pass(pool):
+        futs = []
+        for f64, nv, a in work:
+            chunk = max(1, nv // threads)
+            for v0 in range(0, nv, chunk):
+                futs.append(pool.submit(run_one, f64, a, v0, min(nv, v0 + chunk)))
+        for f in futs:
+            f.result()
+
+    with ThreadPoolExecutor(max_workers=threads) as pool:
+        one_pass(pool)
+        t = time.perf_counter()
+        reps = 0
+        while time.perf_counter() - t < seconds_budget:
+            one_pass(pool)
+            reps += 1
+        el = time.perf_counter() - t
+    return {"value": round(bytes_one * reps / el / 1e9, 3), "unit": "GB/s", "cores": threads,
+            "kind": "reference",
+            "sample": f"first {sample_vecs} vectors of the f64 and f32 ALP columns, alp::decode "
+                      f"(falp + patch, src/alp/alp-bindings.cu) per thread range, {reps} passes "
+                      f"in {el:.1f} s"}
+
+
 def extended_of(col, dev):
     """The ALP-extended (lane-divided) form of an f64 ALP DeviceColumn, built
     on the device as the reference's host-side conversion does
@@ -492,7 +558,8 @@ def run_alp(args, rank, world, dev):
     x_bytes = cols[0][3] - cols[0][1].n_vecs * 2 + x_extra + cols[0][4]
     per["alp_f64_extended"] = {"gbs": round(x_bytes / (x_ms / 1e3) / 1e9, 1), "ms": round(x_ms, 4),
                                "bit_exact": x_exact, "in_headline": False}
-    return dict(gbs=bytes_step * args.steps * world / (ms / 1e3) / 1e9, ms=ms,
+    cpu = cpu_reference_alp(cols, args.cpu_seconds / 2) if rank == 0 and world == 1 else None
+    return dict(gbs=bytes_step * args.steps * world / (ms / 1e3) / 1e9, ms=ms, cpu=cpu,
                 bytes_step=bytes_step, per=per, achieved=bytes_step / (kern_ms / 1e3) / 1e9,
                 launches=launches, clocks=clk.summary(), gen_s=gen_s,
                 exact=all(exact.values()) and x_exact)
@@ -861,6 +928,13 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
+        if args.workload not in ("ffor", "ffor-sum"):
+            print(json.dumps({"impl": "reference", "unavailable":
+                              "the reference arm runs the FFOR workload; the alp and learned "
+                              "workloads carry the reference's CPU ALP decoder / rowgroup "
+                              "encoder in their cpu_baseline, and the reference has no batched "
+                              "decode, pair query or autotuner to run"}))
+            return
         res = cpu_reference_ffor(args.cpu_seconds)
         steps_ms = []
         line = {"impl": "reference", "metric": metric, "value": res["value"], "unit": "GB/s",
@@ -956,6 +1030,7 @@ def main():
                              "traffic": profiled_traffic("alp_decode_at_scale.md",
                                                          r["bytes_step"] / 3),
                              "traffic_source": "profiles/alp_decode_at_scale.md (ncu, one pass)"},
+                "cpu_baseline": r["cpu"],
                 "gpu_launches": r["launches"], "clocks": r["clocks"],
                 "generation_s": round(r["gen_s"], 1)}))
         return
