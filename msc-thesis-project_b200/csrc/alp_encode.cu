@@ -99,10 +99,10 @@ __device__ __forceinline__ int sample_estimate(double s, int e, int f, bool skip
 // the ALP-RD limit 48 * 32; without any pair that round-trips at least two
 // samples the result is pair (0, 0) at the initial estimate, as the scan's.
 __device__ int plain_search(const double *smp, int t, int *est_out, int *pair_out = nullptr) {
-  constexpr int P = 3;  // pairs per round; two rounds cover ceil(190 / 32) = 6
+  constexpr int P = 2;  // pairs per round; three rounds cover ceil(190 / 32) = 6
   uint32_t key = 0xFFFFFFFFu;
 #pragma unroll 1
-  for (int round = 0; round < 2; ++round) {
+  for (int round = 0; round < 3; ++round) {
     // per pair: 10^e, 10^-f, 10^f (as a double) and 10^-e in registers
     // (lanes index the constant tables differently, so they are read once)
     double m10e[P], mfrf[P], factd[P], frce[P], dmn[P], dmx[P];
@@ -124,7 +124,7 @@ __device__ int plain_search(const double *smp, int t, int *est_out, int *pair_ou
       mx[i] = INT64_MIN;
       cnt[i] = 0;
     }
-#pragma unroll 2
+#pragma unroll 4
     for (int k = 0; k < 32; ++k) {
       const double x = smp[k];
 #pragma unroll
@@ -184,7 +184,7 @@ __device__ int plain_search(const double *smp, int t, int *est_out, int *pair_ou
 }
 
 // Labels (the plain search's class) of every vector: one warp per vector.
-__global__ void __launch_bounds__(256) k_plain_labels(const double *__restrict__ vals,
+__global__ void __launch_bounds__(256, 4) k_plain_labels(const double *__restrict__ vals,
                                                       size_t n_vecs, int16_t *labels,
                                                       int32_t *est) {
   const int t = threadIdx.x & 31;

@@ -41,25 +41,63 @@ __device__ __forceinline__ float warp_max_f(float x) {
   return x;
 }
 
+// Bit planes: pl[k] = ballot(bit k of the lane's value).  plane_eq gives the
+// lanes whose value equals `want`, plane_le those whose value is <= `want`;
+// `want` differs per lane, so every lane counts its own histogram bin from
+// the same few ballots instead of one ballot per bin.
+template <int NB>
+__device__ __forceinline__ uint32_t plane_eq(const uint32_t (&pl)[NB], uint32_t want) {
+  uint32_t m = 0xffffffffu;
+#pragma unroll
+  for (int k = 0; k < NB; ++k) m &= ((want >> k) & 1u) ? pl[k] : ~pl[k];
+  return m;
+}
+template <int NB>
+__device__ __forceinline__ uint32_t plane_le(const uint32_t (&pl)[NB], uint32_t want) {
+  uint32_t lt = 0, eq = 0xffffffffu;
+#pragma unroll
+  for (int k = NB - 1; k >= 0; --k) {
+    const uint32_t b = (want >> k) & 1u;
+    lt |= b ? (eq & ~pl[k]) : 0u;
+    eq &= b ? pl[k] : ~pl[k];
+  }
+  return lt | eq;
+}
+// Order-preserving map of floats to unsigned keys (for integer warp min/max).
+__device__ __forceinline__ uint32_t f_key(float f) {
+  const uint32_t b = __float_as_uint(f);
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float f_unkey(uint32_t k) {
+  return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+// A count below 2^23 as a float without a conversion instruction.
+__device__ __forceinline__ float count_f(uint32_t c) {
+  return __uint_as_float(0x4B000000u | c) - 8388608.0f;
+}
+
 // 64 features of a vector from its 32 samples (lane i holds value 32 i, the
-// samples the search uses): magnitude moments, sign / zero / non-finite
-// fractions, histograms of the decimal digits after the point (smallest d
-// with x * 10^d integral), of trailing zero bits of the mantissa, of
-// log10|x|, and of the binary exponent.
-// Lane t receives features t and t + 32 (lo[r], hi[r]) of R vectors at once
-// (x[r] is the lane's sample of vector r): the R computations are
-// independent straight-line code, so they interleave; each feature is
-// selected into lo / hi as it is computed instead of being held in an
-// array.
+// samples the search uses):
+//   0..3   mean, deviation, min, max of log10|x| over the nonzero samples, / 10
+//   4..6   fractions of zeros, negatives, non-finite samples
+//   7..24  histogram of the decimal digits after the point (the smallest
+//          d < 17 with x * 10^d integral, 17 when none)
+//   25..41 histogram of trailing zero bits of the mantissa (/ 4; 16: none)
+//   42..49 histogram of log10|x| in bins of 4 from -12
+//   50..52 mean (/ 17 / 32 summed), max, min of the digits / 17
+//   53     fraction with no digits after the point
+//   54..57 mean, deviation of the binary exponent / 64; min, max / 1024
+//   58..63 fractions with at most 2, 4, .., 12 digits after the point
+// Lane t returns features t and t + 32 (lo[r], hi[r]) of R vectors at once
+// (x[r] is the lane's sample of vector r), so the R computations interleave.
+// Histogram bins come from bit-plane ballots and the integer statistics
+// from warp integer reductions (each lane evaluates only its own two
+// features); the floating-point sums keep a fixed shuffle order, so the
+// training and the inference kernels see identical features.
 template <int R>
 __device__ __forceinline__ void vector_features(const double (&x)[R], int t, float (&lo)[R],
                                                 float (&hi)[R]) {
-  auto put = [&](int r, int j, float v) {
-    lo[r] = (t == j) ? v : lo[r];
-    hi[r] = (t + 32 == j) ? v : hi[r];
-  };
-#pragma unroll
-  for (int r = 0; r < R; ++r) lo[r] = hi[r] = 0.0f;
+  constexpr uint32_t kAll = 0xffffffffu;
   float l[R];
   int d[R], tz[R], e2[R];
   bool fin[R], nz[R];
@@ -76,14 +114,7 @@ __device__ __forceinline__ void vector_features(const double (&x)[R], int t, flo
     l[r] = !nz[r] ? 0.0f
                   : ef ? __log10f(mant) + (float)(ef - 1023) * 0.30102999566f
                        : (float)log10(a);
-    // decimal digits after the point: the smallest dd < 17 with x * 10^dd
-    // integral (17 when none), without a data-dependent loop exit
     d[r] = 17;
-#pragma unroll
-    for (int dd = 0; dd < 17; ++dd) {
-      const double y = __dmul_rn(x[r], c_pow10_feat[dd]);
-      if (d[r] == 17 && fin[r] && fabs(y) < 9007199254740992.0 && y == rint(y)) d[r] = dd;
-    }
     tz[r] = 53;
     if (nz[r]) {
       uint64_t mt = bits & 0xFFFFFFFFFFFFFull;
@@ -92,45 +123,77 @@ __device__ __forceinline__ void vector_features(const double (&x)[R], int t, flo
     }
     e2[r] = (int)((bits >> 52) & 0x7FF) - 1023;
   }
+  // decimal digits after the point: the smallest dd < 17 with x * 10^dd
+  // integral (17 when none, and for non-finite x); the scan stops once
+  // every lane of the warp has its answer (most columns have few digits)
+  {
+    bool pend[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) pend[r] = fin[r];
+#pragma unroll 1
+    for (int dd = 0; dd < 17; ++dd) {
+      const double p10 = c_pow10_feat[dd];
+      bool any = false;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const double y = __dmul_rn(x[r], p10);
+        if (pend[r] && fabs(y) < 9007199254740992.0 && y == rint(y)) {
+          d[r] = dd;
+          pend[r] = false;
+        }
+        any |= pend[r];
+      }
+      if (!__any_sync(kAll, any)) break;
+    }
+  }
 #pragma unroll
   for (int r = 0; r < R; ++r) {
-    const float nnz = (float)__popc(__ballot_sync(0xffffffffu, nz[r]));
-    const float inv = nnz > 0 ? 1.0f / nnz : 0.0f;
+    const uint32_t bnz = __ballot_sync(kAll, nz[r]);
+    const uint32_t bzero = __ballot_sync(kAll, fin[r] && x[r] == 0.0);
+    const uint32_t bneg = __ballot_sync(kAll, fin[r] && x[r] < 0.0);
+    const uint32_t binf = __ballot_sync(kAll, !fin[r]);
+    const uint32_t tzb = tz[r] >= 53 ? 16u : (uint32_t)min(15, tz[r] / 4);
+    const uint32_t lb = (uint32_t)max(0, min(7, __float2int_rd((l[r] + 12.0f) * 0.25f)));
+    uint32_t pd[5], pt[5], pm[3];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      pd[k] = __ballot_sync(kAll, ((uint32_t)d[r] >> k) & 1u);
+      pt[k] = __ballot_sync(kAll, (tzb >> k) & 1u);
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) pm[k] = __ballot_sync(kAll, (lb >> k) & 1u);
+    // the lane's count features: lo slot t, hi slot 32 + t
+    uint32_t mlo = t < 25 ? plane_eq(pd, (uint32_t)(t - 7)) : plane_eq(pt, (uint32_t)(t - 25));
+    mlo = t == 4 ? bzero : t == 5 ? bneg : t == 6 ? binf : mlo;
+    uint32_t mhi = t < 10 ? plane_eq(pt, (uint32_t)(t + 7)) : (plane_eq(pm, (uint32_t)(t - 10)) & bnz);
+    mhi = t == 21 ? plane_eq(pd, 0u) : mhi;
+    mhi = t >= 26 ? plane_le(pd, (uint32_t)(2 + 2 * (t - 26))) : mhi;
+
+    // magnitude statistics over the nonzero samples
+    const uint32_t nnzi = __popc(bnz);
+    const float inv = nnzi > 0 ? 1.0f / count_f(nnzi) : 0.0f;
     const float mean_l = warp_sum_f(nz[r] ? l[r] : 0.0f) * inv;
     const float var_l = warp_sum_f(nz[r] ? (l[r] - mean_l) * (l[r] - mean_l) : 0.0f) * inv;
-    put(r, 0, mean_l / 10.0f);
-    put(r, 1, sqrtf(var_l) / 10.0f);
-    put(r, 2, nnz > 0 ? warp_min_f(nz[r] ? l[r] : 1e30f) / 10.0f : 0.0f);
-    put(r, 3, nnz > 0 ? warp_max_f(nz[r] ? l[r] : -1e30f) / 10.0f : 0.0f);
-    const double a = fabs(x[r]);
-    put(r, 4, __popc(__ballot_sync(0xffffffffu, fin[r] && a == 0.0)) / 32.0f);
-    put(r, 5, __popc(__ballot_sync(0xffffffffu, fin[r] && x[r] < 0.0)) / 32.0f);
-    put(r, 6, __popc(__ballot_sync(0xffffffffu, !fin[r])) / 32.0f);
-    float f7 = 0.0f;
-#pragma unroll
-    for (int b = 0; b < 18; ++b) {
-      const float v = __popc(__ballot_sync(0xffffffffu, d[r] == b)) / 32.0f;
-      if (b == 0) f7 = v;
-      put(r, 7 + b, v);
-    }
-    const int tzb = tz[r] >= 53 ? 16 : min(15, tz[r] / 4);
-#pragma unroll
-    for (int b = 0; b < 17; ++b) put(r, 25 + b, __popc(__ballot_sync(0xffffffffu, tzb == b)) / 32.0f);
-    const int lb = nz[r] ? max(0, min(7, (int)floorf((l[r] + 12.0f) / 4.0f))) : -1;
-#pragma unroll
-    for (int b = 0; b < 8; ++b) put(r, 42 + b, __popc(__ballot_sync(0xffffffffu, lb == b)) / 32.0f);
-    put(r, 50, warp_sum_f((float)d[r]) / (32.0f * 17.0f));
-    put(r, 51, warp_max_f((float)d[r]) / 17.0f);
-    put(r, 52, warp_min_f((float)d[r]) / 17.0f);
-    put(r, 53, f7);
-    const float me = warp_sum_f((float)e2[r]) / 32.0f;
-    put(r, 54, me / 64.0f);
-    put(r, 55, sqrtf(warp_sum_f(((float)e2[r] - me) * ((float)e2[r] - me)) / 32.0f) / 64.0f);
-    put(r, 56, warp_min_f((float)e2[r]) / 1024.0f);
-    put(r, 57, warp_max_f((float)e2[r]) / 1024.0f);
-#pragma unroll
-    for (int jj = 0; jj < 6; ++jj)
-      put(r, 58 + jj, __popc(__ballot_sync(0xffffffffu, d[r] <= 2 + 2 * jj)) / 32.0f);
+    const float lmin = f_unkey(__reduce_min_sync(kAll, nz[r] ? f_key(l[r]) : 0xffffffffu));
+    const float lmax = f_unkey(__reduce_max_sync(kAll, nz[r] ? f_key(l[r]) : 0u));
+    float num = t == 0 ? mean_l : t == 1 ? sqrtf(var_l) : t == 2 ? lmin : lmax;
+    if (nnzi == 0 && t >= 2) num = 0.0f;
+    lo[r] = t < 4 ? num / 10.0f : count_f(__popc(mlo)) * (1.0f / 32.0f);
+
+    // digit and binary-exponent statistics (sums of small integers: exact)
+    const int dsum = __reduce_add_sync(kAll, d[r]);
+    const int dmax = __reduce_max_sync(kAll, d[r]);
+    const int dmin = __reduce_min_sync(kAll, d[r]);
+    const int esum = __reduce_add_sync(kAll, e2[r]);
+    const int emin = __reduce_min_sync(kAll, e2[r]);
+    const int emax = __reduce_max_sync(kAll, e2[r]);
+    const float me = (float)esum / 32.0f;
+    const float esd = sqrtf(warp_sum_f(((float)e2[r] - me) * ((float)e2[r] - me)) / 32.0f);
+    const int ival = t == 18 ? dsum : t == 19 ? dmax : t == 20 ? dmin : t == 24 ? emin : emax;
+    const float den = t == 18 ? 32.0f * 17.0f : t <= 20 ? 17.0f : 1024.0f;
+    const float stat = t == 22 ? me / 64.0f : t == 23 ? esd / 64.0f : (float)ival / den;
+    const bool hcount = t <= 17 || t == 21 || t >= 26;
+    hi[r] = hcount ? count_f(__popc(mhi)) * (1.0f / 32.0f) : stat;
   }
 }
 
@@ -150,26 +213,35 @@ __global__ void __launch_bounds__(256) k_features(const double *__restrict__ val
 using bf16 = __nv_bfloat16;
 
 // ---- fused inference ------------------------------------------------------
-// Features -> three layers -> top-k candidates of 128 vectors per step in
-// one persistent kernel (16 warps, one CTA per SM).  The bf16 weights are
-// staged once per CTA in shared memory in the canonical K-major layout.  Per
-// tile (row r = vector m0 + r): each warp computes the features of 8 rows
-// into the activation tile; one thread issues the MMAs of a layer
-// (tcgen05, FP32 accumulators in tensor memory: layers 1 and 3 at columns
-// 0.., layer 2 at 128..); warp w reads back tensor-memory lanes 32 (w % 4)
-// .. +31 (those rows) for column quarter w / 4, adding bias + ReLU into the
-// next activation tile, or, after layer 3, keeping the top-k of its quarter
-// of the logits, which warps 0..3 merge per row.  The arithmetic is the
+// Features -> three layers -> top-k candidates of 128 vectors per tile in
+// one persistent kernel (32 warps, one CTA per SM).  The bf16 weights are
+// staged once per CTA in shared memory in the canonical K-major layout.  The
+// CTA holds two teams of 16 warps, each with its own tile, activation tile,
+// 256 tensor-memory columns, mbarrier and named barrier, so one team's
+// feature arithmetic overlaps the other's MMAs and waits.  Per tile (row r =
+// vector m0 + r): each warp of the team computes the features of 8 rows
+// into the activation tile; one thread issues the MMAs of a layer (tcgen05,
+// FP32 accumulators in tensor memory: layers 1 and 3 at columns 0.., layer
+// 2 at 128..); warp w reads back tensor-memory lanes 32 (w % 4) .. +31
+// (those rows) for column group (w % 16) / 4, adding bias + ReLU into the
+// next activation tile, or, after layer 3, keeping the top-k of its group's
+// logits, which the team's warps 0..3 merge per row.  The arithmetic is the
 // layer-by-layer path's (the same MMAs in the same K order, bf16
 // activations, fp32 logits, ties to the lower class), so the candidates are
 // the same.
 constexpr int kPropRows = 128;
 constexpr int kPropThreads = 1024;
-constexpr int kPropGroups = kPropThreads / kPropRows;  // column groups per row
+constexpr int kPropTeams = 2;                                 // tiles in flight per CTA
+constexpr int kTeamThreads = kPropThreads / kPropTeams;       // 16 warps
+constexpr int kPropGroups = kTeamThreads / kPropRows;         // column groups per row
 constexpr int kTopMax = 4;
 constexpr size_t kPropSmem =
-    (size_t)(kHidden * kFeatures + kHidden * kHidden + kOut * kHidden + kPropRows * kHidden) * 2 +
-    (size_t)(kHidden + kHidden + kOut) * 4 + (size_t)kPropGroups * kPropRows * kTopMax * (4 + 4);
+    (size_t)(kHidden * kFeatures + kHidden * kHidden + kOut * kHidden +
+             kPropTeams * kPropRows * kHidden) * 2 +
+    (size_t)(kHidden + kHidden + kOut) * 4 +
+    (size_t)kPropTeams * kPropGroups * kPropRows * kTopMax * (4 + 4);
+static_assert(kPropSmem + 1024 <= 227 * 1024, "fused proposal: shared memory of one CTA");
+static_assert(kPropTeams * 256 <= 512, "fused proposal: tensor-memory columns");
 
 __device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8]) {
   asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
@@ -242,26 +314,47 @@ __device__ __forceinline__ void top_insert(float (&bv)[kTopMax], int (&bc)[kTopM
   }
 }
 
+// Barrier of one team (named barrier 1 + team over its threads); team_any
+// also returns whether any of them passed true.
+__device__ __forceinline__ void team_sync(int team) {
+  asm volatile("bar.sync %0, %1;" ::"r"(team + 1), "r"(kTeamThreads) : "memory");
+}
+__device__ __forceinline__ bool team_any(int team, bool v) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.or.pred q, %2, %3, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}\n"
+      : "=r"(r)
+      : "r"((uint32_t)v), "r"(team + 1), "r"(kTeamThreads)
+      : "memory");
+  return r != 0;
+}
+
 __global__ void __launch_bounds__(kPropThreads, 1)
     k_propose(const double *__restrict__ vals, size_t n_vecs, const bf16 *__restrict__ w1,
               const bf16 *__restrict__ w2, const bf16 *__restrict__ w3,
               const float *__restrict__ b1, const float *__restrict__ b2,
               const float *__restrict__ b3, int k, int16_t *cand, uint32_t *status) {
   extern __shared__ __align__(128) unsigned char smem[];
-  __shared__ __align__(8) uint64_t mbar;
+  __shared__ __align__(8) uint64_t mbar[kPropTeams];
   __shared__ uint32_t tmem_slot;
   unsigned char *sW1 = smem;
   unsigned char *sW2 = sW1 + kHidden * kFeatures * 2;
   unsigned char *sW3 = sW2 + kHidden * kHidden * 2;
-  unsigned char *sA = sW3 + kOut * kHidden * 2;
-  float *sb1 = reinterpret_cast<float *>(sA + kPropRows * kHidden * 2);
+  unsigned char *sA0 = sW3 + kOut * kHidden * 2;  // [teams][128 x 128 bf16]
+  float *sb1 = reinterpret_cast<float *>(sA0 + kPropTeams * kPropRows * kHidden * 2);
   float *sb2 = sb1 + kHidden;
   float *sb3 = sb2 + kHidden;
-  float *s_topv = sb3 + kOut;  // [column groups][128][kTopMax]
-  int *s_topc = reinterpret_cast<int *>(s_topv + kPropGroups * kPropRows * kTopMax);
+  float *s_topv0 = sb3 + kOut;  // [teams][column groups][128][kTopMax]
+  int *s_topc0 = reinterpret_cast<int *>(s_topv0 + kPropTeams * kPropGroups * kPropRows * kTopMax);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int lanes = 32 * (warp & 3), quarter = warp >> 2, row = lanes + lane;  // quarter: column group
-  constexpr uint32_t kCols = 256;
+  constexpr int kTeamWarps = kTeamThreads / 32;
+  const int team = warp / kTeamWarps, tw = warp % kTeamWarps;
+  // tensor-memory lanes 32 (warp % 4) .. +31 are the ones this warp may read
+  const int lanes = 32 * (tw & 3), quarter = tw >> 2, row = lanes + lane;  // quarter: column group
+  constexpr uint32_t kCols = 256 * kPropTeams;
 
   // weights and biases, once per CTA
   for (int i = tid; i < kHidden * kFeatures / 8; i += kPropThreads) {
@@ -290,25 +383,33 @@ __global__ void __launch_bounds__(kPropThreads, 1)
                  "r"(kCols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
-  if (tid == 0) asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&mbar)), "r"(1));
+  if (tid < kPropTeams)
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&mbar[tid])), "r"(1));
   asm volatile("tcgen05.fence::before_thread_sync;");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;");
-  const uint32_t tmem = tmem_slot;
+  // this team's accumulators (256 columns), activation tile, top-k scratch
+  const uint32_t tmem = tmem_slot + 256u * (uint32_t)team;
+  unsigned char *sA = sA0 + team * (kPropRows * kHidden * 2);
+  float *s_topv = s_topv0 + team * (kPropGroups * kPropRows * kTopMax);
+  int *s_topc = s_topc0 + team * (kPropGroups * kPropRows * kTopMax);
+  uint64_t *mb = &mbar[team];
+  const bool issuer = tw == 0 && lane == 0;
   const uint32_t aA = smem_u32(sA), aW1 = smem_u32(sW1), aW2 = smem_u32(sW2), aW3 = smem_u32(sW3);
   uint32_t phase = 0;
   bool failed = false;
   const size_t n_tiles = (n_vecs + kPropRows - 1) / kPropRows;
-  constexpr int kRowsPerWarp = kPropRows / (kPropThreads / 32);
+  constexpr int kRowsPerWarp = kPropRows / kTeamWarps;
 
-  for (size_t tile = blockIdx.x; tile < n_tiles && !failed; tile += gridDim.x) {
+  for (size_t tile = (size_t)blockIdx.x * kPropTeams + team; tile < n_tiles && !failed;
+       tile += (size_t)gridDim.x * kPropTeams) {
     const size_t m0 = tile * kPropRows;
-    // features of this warp's 8 rows: lane j loads sample j of all of them
-    // first (one round trip), then the warp works through them
+    // features of this warp's rows: lane j loads sample j of all of them
+    // first (one round trip), then the warp works through them in pairs
     double xs[kRowsPerWarp];
 #pragma unroll
     for (int i = 0; i < kRowsPerWarp; ++i) {
-      const size_t v = m0 + warp * kRowsPerWarp + i;
+      const size_t v = m0 + tw * kRowsPerWarp + i;
       xs[i] = v < n_vecs ? vals[v * VEC + 32 * lane] : 0.0;
     }
 #pragma unroll
@@ -318,7 +419,7 @@ __global__ void __launch_bounds__(kPropThreads, 1)
       vector_features<2>(x2, lane, lo, hi);
 #pragma unroll
       for (int q = 0; q < 2; ++q) {
-        const int r = warp * kRowsPerWarp + i + q;
+        const int r = tw * kRowsPerWarp + i + q;
         *reinterpret_cast<bf16 *>(sA + canon_off(r, lane, kPropRows)) = __float2bfloat16_rn(lo[q]);
         *reinterpret_cast<bf16 *>(sA + canon_off(r, lane + 32, kPropRows)) =
             __float2bfloat16_rn(hi[q]);
@@ -326,10 +427,10 @@ __global__ void __launch_bounds__(kPropThreads, 1)
     }
     asm volatile("fence.proxy.async.shared::cta;");
     asm volatile("tcgen05.fence::before_thread_sync;");
-    __syncthreads();
+    team_sync(team);
     // layer 1 -> columns 0..127
-    if (tid == 0) issue_layer(tmem, aA, aW1, kHidden, kFeatures, &mbar);
-    if (__syncthreads_or(!mbar_wait(&mbar, phase))) {
+    if (issuer) issue_layer(tmem, aA, aW1, kHidden, kFeatures, mb);
+    if (team_any(team, !mbar_wait(mb, phase))) {
       failed = true;
       break;
     }
@@ -338,10 +439,10 @@ __global__ void __launch_bounds__(kPropThreads, 1)
     hidden_epilogue(tmem, lanes, quarter, row, 0, sb1, sA);
     asm volatile("fence.proxy.async.shared::cta;");
     asm volatile("tcgen05.fence::before_thread_sync;");
-    __syncthreads();
+    team_sync(team);
     // layer 2 -> columns 128..255
-    if (tid == 0) issue_layer(tmem + 128, aA, aW2, kHidden, kHidden, &mbar);
-    if (__syncthreads_or(!mbar_wait(&mbar, phase))) {
+    if (issuer) issue_layer(tmem + 128, aA, aW2, kHidden, kHidden, mb);
+    if (team_any(team, !mbar_wait(mb, phase))) {
       failed = true;
       break;
     }
@@ -350,10 +451,10 @@ __global__ void __launch_bounds__(kPropThreads, 1)
     hidden_epilogue(tmem, lanes, quarter, row, 128, sb2, sA);
     asm volatile("fence.proxy.async.shared::cta;");
     asm volatile("tcgen05.fence::before_thread_sync;");
-    __syncthreads();
+    team_sync(team);
     // layer 3 -> columns 0..191
-    if (tid == 0) issue_layer(tmem, aA, aW3, kOut, kHidden, &mbar);
-    if (__syncthreads_or(!mbar_wait(&mbar, phase))) {
+    if (issuer) issue_layer(tmem, aA, aW3, kOut, kHidden, mb);
+    if (team_any(team, !mbar_wait(mb, phase))) {
       failed = true;
       break;
     }
@@ -388,9 +489,9 @@ __global__ void __launch_bounds__(kPropThreads, 1)
       }
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
-    __syncthreads();
+    team_sync(team);
     if (quarter == 0) {
-      // merge the quarters in class order: a logit equal to one already
+      // merge the groups in class order: a logit equal to one already
       // listed stays behind it
       float bv[kTopMax];
       int bc[kTopMax];
@@ -399,6 +500,7 @@ __global__ void __launch_bounds__(kPropThreads, 1)
         bv[q] = s_topv[row * kTopMax + q];
         bc[q] = s_topc[row * kTopMax + q];
       }
+#pragma unroll
       for (int qq = 1; qq < kPropGroups; ++qq)
 #pragma unroll
         for (int q = 0; q < kTopMax; ++q)
@@ -409,16 +511,16 @@ __global__ void __launch_bounds__(kPropThreads, 1)
         for (int q = 0; q < k; ++q) cand[v * k + q] = (int16_t)bc[q];
     }
     // the activation tile, the top-k scratch and tensor memory are reused
-    __syncthreads();
+    team_sync(team);
   }
   if (failed) {
-    if (tid == 0 && status) atomicOr(status, 0x100u);
-    mbar_wait(&mbar, phase);  // the MMAs in flight, bounded, before dealloc
+    if (issuer && status) atomicOr(status, 0x100u);
+    mbar_wait(mb, phase);  // the MMAs in flight, bounded, before dealloc
   }
   asm volatile("tcgen05.fence::before_thread_sync;");
   __syncthreads();
   if (warp == 0)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_slot), "r"(kCols));
 }
 
 // Softmax cross entropy over the 191 real classes of each row (class 191
@@ -803,7 +905,8 @@ flsgpu_status propose(flsgpu_alp_encoder *e, const double *vals, size_t n_vecs, 
     attr = true;
   }
   const size_t tiles = (n_vecs + kPropRows - 1) / kPropRows;
-  const unsigned grid = (unsigned)std::min<size_t>(tiles, (size_t)sm_count());
+  const unsigned grid =
+      (unsigned)std::min<size_t>((tiles + kPropTeams - 1) / kPropTeams, (size_t)sm_count());
   k_propose<<<grid, kPropThreads, kPropSmem, s>>>(vals, n_vecs, e->w1b, e->w2b, e->w3b, e->w + kOffB1,
                                                e->w + kOffB2, e->w + kOffB3, k, e->cand, e->status);
   note_launch();
