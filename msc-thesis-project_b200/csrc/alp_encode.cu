@@ -274,46 +274,101 @@ __device__ VecAnalysis analyze_vector(const double *__restrict__ vec, int e, int
   return a;
 }
 
-// Packed words (bw * 16 u64 at `packed`) and exceptions (value, position,
-// ascending position) at `exc` / `pos` of one vector, staged in the warp's
-// shared copy `sv` of the vector (filled and synchronised by the caller);
-// exc_mask is this thread's exception mask from the analysis, so only the
-// non-exceptions are encoded here (no decode, no comparison).
-__device__ void pack_vector(const double *sv, int e, int f, int t, int64_t fill, uint64_t base,
-                            int bw, uint32_t exc_mask, uint64_t *packed, double *exc,
-                            uint16_t *pos) {
-  const int lane = t & 15, half = t >> 4;
-  // this thread's 32 values are bits [32*half*bw, 32*(half+1)*bw) of the
-  // lane stream = its bw 32-bit words, owned by it alone
-  uint32_t *p32 = reinterpret_cast<uint32_t *>(packed) + 2 * lane;
-  const uint64_t mask = bw >= 64 ? ~0ull : ((1ull << bw) - 1);
-  uint32_t acc = 0;  // pending low bits (< 32 of them)
-  int nacc = 0, m = half * bw;
-  if (bw > 0) {
-#pragma unroll 2
-    for (int k = 0; k < 32; ++k) {
-      const int64_t q = ((exc_mask >> k) & 1)
-                            ? fill
-                            : enc_value(sv[lane + 16 * (32 * half + k)], f, e, false);
-      const uint64_t d = ((uint64_t)q - base) & mask;
-      // (hi:lo) = acc | d << nacc, total = nacc + bw bits (at most 95)
-      uint64_t lo = (uint64_t)acc | (d << nacc);
-      uint32_t hi = nacc ? (uint32_t)(d >> (64 - nacc)) : 0u;
-      int total = nacc + bw;
-      while (total >= 32) {
-        p32[(m >> 1) * 32 + (m & 1)] = (uint32_t)lo;
-        ++m;
-        lo = (lo >> 32) | ((uint64_t)hi << 32);
-        hi = 0;
-        total -= 32;
+// The stored integer of a non-exception value: the reference's
+// round-to-integer by adding and subtracting 2^52 + 2^51.  For |t| < 2^51
+// the sum lies in [2^52, 2^53), where its mantissa bits are the integer +
+// 2^51, so the integer is read from the bits (no conversion instruction);
+// larger magnitudes take the conversion.
+__device__ __forceinline__ int64_t enc_stored(double x, double m10e, double mfrf) {
+  const double t = __dmul_rn(__dmul_rn(x, m10e), mfrf);
+  const double s = __dadd_rn(t, kMagic);
+  if (fabs(t) < 2251799813685248.0)
+    return (int64_t)((uint64_t)__double_as_longlong(s) & 0xFFFFFFFFFFFFFull) - 2251799813685248ll;
+  return cvtt_s64(__dsub_rn(s, kMagic));
+}
+
+// The bw 32-bit words of one thread: its 32 values (value k at position
+// lane + 16 (32 half + k)), as offsets from the vector's base, are bits
+// [32 half bw, 32 (half + 1) bw) of the lane's stream, so the words are the
+// thread's alone.  Word m of lane l of the 64-bit stream lives at 32-bit
+// index 2 l + 32 (m / 2) + m % 2, i.e. word w of this thread (m = half bw +
+// w) at 16 m - 15 (m % 2): pa + 16 w for even w, pb + 16 w for odd w.  The
+// values are loaded eight at a time (for each k the warp reads two whole
+// 128-byte lines) and encoded with exceptions storing the fill integer;
+// widths up to 32 take 32-bit shifts only.
+__device__ __forceinline__ void pack_thread(const double *__restrict__ vec, uint32_t mask,
+                                            int64_t fill, uint64_t base, double m10e,
+                                            double mfrf, int bw, uint32_t *p32, int lane,
+                                            int half) {
+  const int oddm0 = half & bw & 1;
+  uint32_t *pa = p32 + half * 16 * bw - (oddm0 ? 15 : 0);
+  uint32_t *pb = p32 + half * 16 * bw - (oddm0 ? 0 : 15);
+  const uint64_t vmask = bw >= 64 ? ~0ull : ((1ull << bw) - 1);
+  const double *src = vec + lane + 16 * 32 * half;
+  int w = 0;         // the next word
+  uint32_t acc = 0;  // its pending low bits
+  int nacc = 0;      // how many
+  if (bw <= 32) {
+#pragma unroll 1
+    for (int c = 0; c < 32; c += 8) {
+      double xv[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) xv[i] = src[16 * (c + i)];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int k = c + i;
+        const int64_t q = ((mask >> k) & 1u) ? fill : enc_stored(xv[i], m10e, mfrf);
+        const uint32_t d = (uint32_t)(((uint64_t)q - base) & vmask);
+        const uint32_t lo = acc | (d << nacc);
+        nacc += bw;
+        if (nacc >= 32) {
+          ((w & 1) ? pb : pa)[16 * w] = lo;
+          ++w;
+          nacc -= 32;
+          acc = nacc ? d >> (bw - nacc) : 0u;  // the bits of d past the word
+        } else {
+          acc = lo;
+        }
       }
-      acc = (uint32_t)lo;
-      nacc = total;
+    }
+  } else {
+#pragma unroll 1
+    for (int c = 0; c < 32; c += 8) {
+      double xv[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) xv[i] = src[16 * (c + i)];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int k = c + i;
+        const int64_t q = ((mask >> k) & 1u) ? fill : enc_stored(xv[i], m10e, mfrf);
+        const uint64_t d = ((uint64_t)q - base) & vmask;
+        // (hi:lo) = acc | d << nacc holds nacc + bw (33..95) bits
+        const uint64_t lo = (uint64_t)acc | (d << nacc);
+        const uint32_t hi = nacc ? (uint32_t)(d >> (64 - nacc)) : 0u;
+        int total = nacc + bw - 32;
+        ((w & 1) ? pb : pa)[16 * w] = (uint32_t)lo;
+        ++w;
+        if (total >= 32) {
+          ((w & 1) ? pb : pa)[16 * w] = (uint32_t)(lo >> 32);
+          ++w;
+          total -= 32;
+          acc = hi;
+        } else {
+          acc = (uint32_t)(lo >> 32);
+        }
+        nacc = total;
+      }
     }
   }
-  // exceptions in ascending position: positions of round r = 16 * r + lane,
-  // rounds 0..31 come from half 0, rounds 32..63 from half 1; only rounds
-  // holding an exception are visited
+}
+
+// Exceptions (value, position) of one vector in ascending position at `exc`
+// / `pos`: positions of round r = 16 r + lane, rounds 0..31 come from half
+// 0, rounds 32..63 from half 1; only rounds holding an exception are
+// visited.  exc_mask is this thread's mask from the analysis.
+__device__ __forceinline__ void write_exceptions(const double *__restrict__ vec, uint32_t exc_mask,
+                                                 int t, double *exc, uint16_t *pos) {
+  const int lane = t & 15, half = t >> 4;
   const uint32_t any0 = __reduce_or_sync(0xffffffffu, half == 0 ? exc_mask : 0u);
   const uint32_t any1 = __reduce_or_sync(0xffffffffu, half == 1 ? exc_mask : 0u);
   uint64_t rounds = (uint64_t)any0 | ((uint64_t)any1 << 32);
@@ -327,7 +382,7 @@ __device__ void pack_vector(const double *sv, int e, int f, int t, int64_t fill,
     if (mine) {
       const int slot = written + __popc(bal & ((1u << t) - 1));
       const int p = lane + 16 * r;
-      exc[slot] = sv[p];
+      exc[slot] = vec[p];
       pos[slot] = (uint16_t)p;
     }
     written += __popc(bal);
@@ -557,31 +612,31 @@ __global__ void __launch_bounds__(1024) k_scan_blocks(size_t nb, size_t *blk_wor
 }
 
 
-// Packing at the final offsets: one warp per vector.
-__global__ void __launch_bounds__(256) k_alp_pack(const double *__restrict__ vals, size_t n_vecs,
+// Packing at the final offsets: one warp per vector; thread t loads its 32
+// values straight from the column and writes its words of the lane stream.
+__global__ void __launch_bounds__(256, 4) k_alp_pack(const double *__restrict__ vals, size_t n_vecs,
                                                   EncodeSlots sl, size_t *off_words,
                                                   size_t *off_exc, const size_t *blk_words,
                                                   const size_t *blk_exc, uint64_t *packed,
                                                   double *exc, uint16_t *pos) {
-  extern __shared__ __align__(16) double s_vec[];  // 1024 doubles per warp
-  double *sv = s_vec + (threadIdx.x >> 5) * VEC;
-  const int t = threadIdx.x & 31;
+  const int t = threadIdx.x & 31, lane = t & 15, half = t >> 4;
   const size_t nw = ((size_t)gridDim.x * blockDim.x) >> 5;
   for (size_t v = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n_vecs; v += nw) {
+    const double *vec = vals + v * VEC;
     const size_t ow = off_words[v] + blk_words[v >> 10], oe = off_exc[v] + blk_exc[v >> 10];
-    // the vector into shared memory: all of its loads in flight at once
-    const double2 *src = reinterpret_cast<const double2 *>(vals + v * VEC);
-    double2 *dst = reinterpret_cast<double2 *>(sv);
-    __syncwarp();
-#pragma unroll
-    for (int i = 0; i < VEC / 64; ++i) dst[t + 32 * i] = src[t + 32 * i];
-    __syncwarp();
+    const int bw = sl.bw[v];
+    const double m10e = c_f64_exp10[sl.exp[v]], mfrf = c_f64_frac[sl.fac[v]];
+    const int64_t fill = sl.fill[v];
+    const uint64_t base = sl.base[v];
+    const uint32_t mask = sl.exc_mask[v * 32 + t];
     if (t == 0) {
       off_words[v] = ow;  // the column's final offsets
       off_exc[v] = oe;
     }
-    pack_vector(sv, sl.exp[v], sl.fac[v], t, sl.fill[v], sl.base[v], sl.bw[v],
-                sl.exc_mask[v * 32 + t], packed + ow, exc + oe, pos + oe);
+    if (bw > 0)
+      pack_thread(vec, mask, fill, base, m10e, mfrf, bw,
+                  reinterpret_cast<uint32_t *>(packed + ow) + 2 * lane, lane, half);
+    write_exceptions(vec, mask, t, exc + oe, pos + oe);
   }
 }
 
@@ -623,12 +678,7 @@ flsgpu_status run_alp_encode(const double *vals, size_t n_vecs, int mode, const 
   k_encode_stats<<<persistent_blocks(n_vecs / 32 + 1, 8, 2), 256, 0, s>>>(sl.flags, sl.bw, n_vecs,
                                                                            totals);
   note_launch();
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_alp_pack, cudaFuncAttributeMaxDynamicSharedMemorySize, 8 * VEC * 8);
-    attr = true;
-  }
-  k_alp_pack<<<warps_grid(n_vecs), 256, 8 * VEC * sizeof(double), s>>>(
+  k_alp_pack<<<warps_grid(n_vecs), 256, 0, s>>>(
       vals, n_vecs, sl, off_words, off_exc, sl.blk_words, sl.blk_exc, packed, exc, pos);
   note_launch(3);
   return check_cuda(cudaGetLastError(), "alp encode");
