@@ -53,6 +53,31 @@ __device__ __forceinline__ double dec_value(int64_t q, int f, int e) {
                    c_f64_frac[e]);
 }
 
+// The stored integer of a non-exception value: the reference's
+// round-to-integer by adding and subtracting 2^52 + 2^51.  For |t| < 2^51
+// the sum lies in [2^52, 2^53), where its mantissa bits are the integer +
+// 2^51, so the integer is read from the bits (no conversion instruction);
+// larger magnitudes take the conversion.
+__device__ __forceinline__ int64_t enc_stored(double x, double m10e, double mfrf) {
+  const double t = __dmul_rn(__dmul_rn(x, m10e), mfrf);
+  const double s = __dadd_rn(t, kMagic);
+  if (fabs(t) < 2251799813685248.0)
+    return (int64_t)((uint64_t)__double_as_longlong(s) & 0xFFFFFFFFFFFFFull) - 2251799813685248ll;
+  return cvtt_s64(__dsub_rn(s, kMagic));
+}
+
+// dec_value with the factor and 10^-e in registers: the wrapped product
+// q * 10^f converted to double through the magic sum when it lies in
+// (-2^51, 2^51) (exact there), by the conversion otherwise.
+__device__ __forceinline__ double dec_stored(int64_t q, uint64_t fact, double frce) {
+  const uint64_t n = (uint64_t)q * fact;
+  const double dn =
+      n + 2251799813685248ull < 4503599627370496ull
+          ? __dsub_rn(__longlong_as_double((long long)(n + 0x4338000000000000ull)), kMagic)
+          : __ll2double_rn((long long)n);
+  return __dmul_rn(dn, frce);
+}
+
 __device__ __forceinline__ int count_bits64(uint64_t x) { return x ? 64 - __clzll((long long)x) : 0; }
 
 __device__ __forceinline__ int64_t warp_max_s64(int64_t x) {
@@ -214,13 +239,14 @@ __global__ void __launch_bounds__(256, 4) k_plain_labels(const double *__restric
 
 // encode_simdized's exception test for one value: specials (inf, NaN,
 // -0.0) are encoded as the upper bound and become exceptions.
-__device__ __forceinline__ int64_t enc_checked(double x, int f, int e, bool *is_exc) {
+__device__ __forceinline__ int64_t enc_checked(double x, double m10e, double mfrf, uint64_t fact,
+                                               double frce, bool *is_exc) {
   const uint64_t bits = (uint64_t)__double_as_longlong(x);
   const bool special = ((bits & 0x7FFFFFFFFFFFFFFFull) >= 0x7FF0000000000000ull) ||
                        bits == 0x8000000000000000ull;
   const double a = special ? kEncUpper : x;
-  const int64_t q = enc_value(a, f, e, false);
-  *is_exc = dec_value(q, f, e) != a;
+  const int64_t q = enc_stored(a, m10e, mfrf);
+  *is_exc = dec_stored(q, fact, frce) != a;
   return q;
 }
 
@@ -237,20 +263,28 @@ __device__ VecAnalysis analyze_vector(const double *__restrict__ vec, int e, int
   uint32_t exc_mask = 0;
   int first_ok = 1 << 30;
   int64_t mn = INT64_MAX, mx = INT64_MIN;
-  // all 32 loads in flight before any use (the kernel is latency-bound)
-  double xv[32];
+  const double m10e = c_f64_exp10[e], mfrf = c_f64_frac[f], frce = c_f64_frac[e];
+  const uint64_t fact = (uint64_t)c_f64_fact[f];
+  const double *src = vec + lane + 16 * 32 * half;
+  // eight loads in flight at a time (each a whole 128-byte line per half
+  // warp), few registers, so that many warps hide the latency
+#pragma unroll 1
+  for (int c = 0; c < 32; c += 8) {
+    double xv[8];
 #pragma unroll
-  for (int k = 0; k < 32; ++k) xv[k] = vec[lane + 16 * (32 * half + k)];
+    for (int i = 0; i < 8; ++i) xv[i] = src[16 * (c + i)];
 #pragma unroll
-  for (int k = 0; k < 32; ++k) {
-    const int p = lane + 16 * (32 * half + k);
-    bool is_exc;
-    const int64_t q = enc_checked(xv[k], f, e, &is_exc);
-    exc_mask |= (uint32_t)is_exc << k;
-    if (!is_exc) {
-      first_ok = min(first_ok, p);
-      mn = q < mn ? q : mn;
-      mx = q > mx ? q : mx;
+    for (int i = 0; i < 8; ++i) {
+      const int k = c + i;
+      const int p = lane + 16 * (32 * half + k);
+      bool is_exc;
+      const int64_t q = enc_checked(xv[i], m10e, mfrf, fact, frce, &is_exc);
+      exc_mask |= (uint32_t)is_exc << k;
+      if (!is_exc) {
+        first_ok = min(first_ok, p);
+        mn = q < mn ? q : mn;
+        mx = q > mx ? q : mx;
+      }
     }
   }
 #pragma unroll
@@ -272,19 +306,6 @@ __device__ VecAnalysis analyze_vector(const double *__restrict__ vec, int e, int
   a.bw = count_bits64((uint64_t)mx - (uint64_t)mn);
   a.base = (uint64_t)mn;
   return a;
-}
-
-// The stored integer of a non-exception value: the reference's
-// round-to-integer by adding and subtracting 2^52 + 2^51.  For |t| < 2^51
-// the sum lies in [2^52, 2^53), where its mantissa bits are the integer +
-// 2^51, so the integer is read from the bits (no conversion instruction);
-// larger magnitudes take the conversion.
-__device__ __forceinline__ int64_t enc_stored(double x, double m10e, double mfrf) {
-  const double t = __dmul_rn(__dmul_rn(x, m10e), mfrf);
-  const double s = __dadd_rn(t, kMagic);
-  if (fabs(t) < 2251799813685248.0)
-    return (int64_t)((uint64_t)__double_as_longlong(s) & 0xFFFFFFFFFFFFFull) - 2251799813685248ll;
-  return cvtt_s64(__dsub_rn(s, kMagic));
 }
 
 // The bw 32-bit words of one thread: its 32 values (value k at position
@@ -396,7 +417,7 @@ __device__ __forceinline__ void write_exceptions(const double *__restrict__ vec,
 // more than `max_exc` exceptions in the vector.  Writes the vector's
 // exponent, factor, width, base, exception count, fill integer and flags
 // (bit 0: the plain search ran as fallback; bit 1: ALP-RD territory).
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 4)
     k_alp_choose(const double *__restrict__ vals, size_t n_vecs, int mode,
                  const int16_t *__restrict__ cand, int k_cand, int max_exc, EncodeSlots sl) {
   __shared__ double s_smp[8][32];
@@ -474,7 +495,7 @@ __global__ void __launch_bounds__(256)
 
 // The plain search and analysis of the vectors k_alp_choose listed (their
 // proposal left more than max_exc exceptions); one warp per listed vector.
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 4)
     k_alp_fallback(const double *__restrict__ vals, EncodeSlots sl) {
   __shared__ double s_smp[8][32];
   double *smp = s_smp[threadIdx.x >> 5];
