@@ -1,11 +1,20 @@
-"""Benchmark: FastLanes FFOR decode at scale on one B200 (the FFOR bit-unpack
-benchmark configuration): one uint32 column of 2^28 values for every bit
-width 0..32 and one uint64 column of 2^27 values for every bit width 0..64,
-values = per-vector base + uniform [0, 2^w).  A step decodes every column
-once into HBM through the library's C ABI.
+"""Benchmark of the B200 FastLanes / ALP decoding library on one B200.
+
+Headline (`value`): FFOR decode at scale (the FFOR bit-unpack benchmark
+configuration): one uint32 column of 2^28 values for every bit width 0..32
+and one uint64 column of 2^27 values for every bit width 0..64, values =
+per-vector base + uniform [0, 2^w).  A step decodes every column once into
+HBM through the library's C ABI.  The default run then measures the rest of
+the benchmark metric in the same invocation, each block with its own clock
+samples: the same columns decoded and summed (`ffor_sum`), ALP / ALP-RD /
+f32 ALP decode (`alp_decode`), 2 000 uneven columns decoded by the batched
+persistent launch against one launch per column plus the pair query
+(`batch_decode`), and the learned ALP encoder against the plain search
+(`learned_encode`).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                    [--workload ffor|ffor-sum|alp] [--scale S]
+                    [--workload ffor|ffor-sum|alp|batch|learned|autotune]
+                    [--scale S] [--no-extras] [--no-e2e]
 
 Prints one JSON line (rank 0).  value = (compressed bytes read + decoded
 bytes written) / device time, whole job.  Inputs are generated on the
@@ -35,6 +44,11 @@ sys.path.insert(0, str(ROOT / "msc-thesis-project_b200"))
 sys.path.insert(0, str(ROOT / "tests"))
 
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+# algorithmic bytes of one headline step (98 FFOR columns, compressed read +
+# decoded write), for relating the bounded e2e sample to the headline
+HEADLINE_STEP_BYTES = sum(
+    (n // 1024) * (w * 128 + b // 8 + 9) + n * b // 8
+    for b, n, ws in ((32, 2 ** 28, range(33)), (64, 2 ** 27, range(65))) for w in ws)
 
 
 def peaks():
@@ -66,6 +80,10 @@ class ClockSampler:
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            # the timed region starts once the sampler is live
+            t0 = time.perf_counter()
+            while not self.lines and time.perf_counter() - t0 < 3.0 and self.proc.poll() is None:
+                time.sleep(0.01)
         except FileNotFoundError:
             self.proc = None
         return self
@@ -162,6 +180,31 @@ def max_over_ranks(x: float, world: int) -> float:
     return float(t.item())
 
 
+def timed_loop(fn, stream, steps: int, warmup: int, min_seconds: float = 1.5):
+    """Mean device time (ms) of fn() over at least `steps` calls and at least
+    min_seconds of device time (so that the clock sampler sees the load),
+    after `warmup` untimed calls; CUDA events on `stream`.  Returns
+    (ms per call, calls timed)."""
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    est = max(e0.elapsed_time(e1), 1e-3)
+    n = max(steps, int(min_seconds * 1e3 / est) + 1)
+    e0.record(stream)
+    for _ in range(n):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / n, n
+
+
 def job_gbs(bytes_per_replica_step: int, steps: int, world: int, max_ms: float) -> float:
     """Whole-job GB/s of `world` replicas each moving bytes_per_replica_step
     per step, timed by the slowest replica."""
@@ -223,6 +266,7 @@ def run_ffor(args, rank, world, dev):
     if args.only:
         only = {(int(t.split(":")[0][1:]), int(t.split(":")[1])) for t in args.only.split(",")}
     cols = make_ffor_columns(args.scale, dev, only)
+    cols_n = range(len(cols))
     out = torch.empty(max(c.n_values for _, _, c in cols) * 8 // 4, dtype=torch.int32, device=dev)
     total_read = sum(col_bytes(c)[0] for _, _, c in cols)
     total_write = sum(col_bytes(c)[1] for _, _, c in cols)
@@ -277,10 +321,56 @@ def run_ffor(args, rank, world, dev):
     # bytes / mean launch duration, over all columns
     kern_ms = sum(statistics.mean(t) for t in per_col_ms)
     achieved = bytes_step / (kern_ms / 1e3) / 1e9
+    fsum_block = run_ffor_sum(args, cols, out, dev) if args.extras and not fsum else None
+    del cols, out
     return dict(gbs=gbs, ms=ms, bytes_step=bytes_step, read=read_b, write=write_b,
                 per_width=per_width, achieved=achieved, launches=launches, clocks=clk.summary(),
                 uncompressed_gbs=total_write * args.steps * world / (ms / 1e3) / 1e9,
-                n_columns=len(cols))
+                n_columns=len(cols_n), fsum=fsum_block)
+
+
+def run_ffor_sum(args, cols, out, dev):
+    """The FFOR-at-scale columns decoded and summed (the fused-reduction
+    kernel, flsgpu_sum_ffor_u32/u64; sums exact mod 2^64), and a full-size
+    parity check of the sums of a few columns against a torch sum of the
+    same columns' decoded output."""
+    import torch
+    import flsgpu_b200 as F
+    stream = torch.cuda.current_stream()
+    sums = torch.zeros(len(cols), dtype=torch.int64, device=dev)
+
+    def step():
+        for i, (bits, w, c) in enumerate(cols):
+            F.sum_(c, out=sums[i:i + 1], stream=stream)
+
+    launches0 = F.launch_count()
+    step()
+    torch.cuda.synchronize()
+    launches = F.launch_count() - launches0
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        ms, n = timed_loop(step, stream, args.steps, args.warmup)
+    exact = {}
+    for i, (bits, w, c) in enumerate(cols):
+        if (bits, w) not in ((32, 7), (32, 32), (64, 1), (64, 40), (64, 64)):
+            continue
+        o = out.view(torch.int64 if bits == 64 else torch.int32)[:c.n_values]
+        F.decompress(c, out=o, stream=stream)
+        ref = (o.to(torch.int64) & 0xFFFFFFFF).sum() if bits == 32 else o.sum()
+        exact[f"u{bits}_w{w}"] = bool(int(ref.item()) == int(sums[i].item()))
+    read = sum(col_bytes(c)[0] for _, _, c in cols)
+    decoded = sum(col_bytes(c)[1] for _, _, c in cols)
+    pk, pk_kind = peaks()
+    hbm = float(pk["hbm_gbs"])
+    gbs = (read + 8 * len(cols)) / (ms / 1e3) / 1e9
+    return {"metric": "FFOR decode fused with a sum: GB/s of compressed bytes read + 8 B per column",
+            "value": round(gbs, 1), "unit": "GB/s", f"frac_of_{pk_kind}": round(gbs / hbm, 4),
+            "decoded_equivalent_gbs": round(decoded / (ms / 1e3) / 1e9, 1),
+            "ms_per_step": round(ms, 3), "steps": n, "columns": len(cols),
+            "kernel": "k_column<T, FFOR, S_SUM> (flsgpu_sum_ffor_u32/u64)",
+            "issue_bound_note": "at low widths the unpack-and-add of 2^28 values per column, not "
+                                "the compressed reads, bounds the kernel",
+            "sum_exact_vs_decoded": exact, "gpu_launches_per_step": launches,
+            "clocks": clk.summary()}
 
 
 # ---------------------------------------------------------------------------
@@ -513,16 +603,23 @@ def run_alp(args, rank, world, dev):
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
+    # enough steps for at least 1.5 s of device time (a step is ~1 ms), so
+    # that the clock sampler sees the load
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    steps = max(args.steps, int(1500.0 / max(e0.elapsed_time(e1), 1e-3)) + 1)
     events = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-               for _ in cols] for _ in range(args.steps)]
+               for _ in cols] for _ in range(steps)]
     launches0 = F.launch_count()
     barrier(world)
     torch.cuda.synchronize()
     with ClockSampler(torch.cuda.current_device()) as clk:
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        for st in range(args.steps):
+        for st in range(steps):
             step(events[st])
         e1.record(stream)
         torch.cuda.synchronize()
@@ -531,11 +628,14 @@ def run_alp(args, rank, world, dev):
     ms = max_over_ranks(e0.elapsed_time(e1), world)
     per = {}
     kern_ms = 0.0
+    pk, pk_kind = peaks()
+    hbm = float(pk["hbm_gbs"])
     for i, (name, c, v, rb, wb) in enumerate(cols):
         t = statistics.mean(events[st][i][0].elapsed_time(events[st][i][1])
-                            for st in range(args.steps))
+                            for st in range(steps))
         kern_ms += t
-        per[name] = {"gbs": round((rb + wb) / (t / 1e3) / 1e9, 1), "ms": round(t, 4),
+        gbs = (rb + wb) / (t / 1e3) / 1e9
+        per[name] = {"gbs": round(gbs, 1), "ms": round(t, 4), f"frac_of_{pk_kind}": round(gbs / hbm, 4),
                      "read_bytes": rb, "write_bytes": wb, "bit_exact": exact[name],
                      "values": c.n_values}
     bytes_step = sum(rb + wb for _, _, _, rb, wb in cols)
@@ -547,19 +647,17 @@ def run_alp(args, rank, world, dev):
     x_exact = bool(torch.equal(xo.view(torch.int64), cols[0][2].view(torch.int64)))
     for _ in range(args.warmup):
         F.decompress(xcol, out=xo, stream=stream)
-    xe0 = torch.cuda.Event(enable_timing=True)
-    xe1 = torch.cuda.Event(enable_timing=True)
-    xe0.record(stream)
-    for _ in range(args.steps):
-        F.decompress(xcol, out=xo, stream=stream)
-    xe1.record(stream)
-    torch.cuda.synchronize()
-    x_ms = xe0.elapsed_time(xe1) / args.steps
+    with ClockSampler(torch.cuda.current_device()) as xclk:
+        x_ms, x_n = timed_loop(lambda: F.decompress(xcol, out=xo, stream=stream), stream,
+                               args.steps, 0)
     x_bytes = cols[0][3] - cols[0][1].n_vecs * 2 + x_extra + cols[0][4]
-    per["alp_f64_extended"] = {"gbs": round(x_bytes / (x_ms / 1e3) / 1e9, 1), "ms": round(x_ms, 4),
-                               "bit_exact": x_exact, "in_headline": False}
+    x_gbs = x_bytes / (x_ms / 1e3) / 1e9
+    per["alp_f64_extended"] = {"gbs": round(x_gbs, 1), "ms": round(x_ms, 4),
+                               f"frac_of_{pk_kind}": round(x_gbs / hbm, 4), "launches_timed": x_n,
+                               "bit_exact": x_exact, "in_headline": False, "clocks": xclk.summary()}
+    del xcol, xo
     cpu = cpu_reference_alp(cols, args.cpu_seconds / 2) if rank == 0 and world == 1 else None
-    return dict(gbs=bytes_step * args.steps * world / (ms / 1e3) / 1e9, ms=ms, cpu=cpu,
+    return dict(gbs=bytes_step * steps * world / (ms / 1e3) / 1e9, ms=ms, cpu=cpu, steps=steps,
                 bytes_step=bytes_step, per=per, achieved=bytes_step / (kern_ms / 1e3) / 1e9,
                 launches=launches, clocks=clk.summary(), gen_s=gen_s,
                 exact=all(exact.values()) and x_exact)
@@ -663,35 +761,48 @@ def run_batch(args, dev):
     read_b = sum(c.compressed_bytes() for c in cols)
     write_b = sum(o.numel() * o.element_size() for o in outs)
 
-    def timed(fn, steps, warm):
-        for _ in range(warm):
-            fn()
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(steps):
-            fn()
-        e1.record(stream)
-        torch.cuda.synchronize()
-        return e0.elapsed_time(e1) / steps
+    def checksums():
+        """Per-column checksum of the decoded bit patterns (wrapping int64
+        sum), to compare the batched decode with per-column decodes."""
+        return torch.stack([(o.view(torch.int32) if o.element_size() == 4 else o.view(torch.int64))
+                            .to(torch.int64).sum() for o in outs])
 
     b.capture(stream)
     launches0 = F.launch_count()
+    b.replay(stream)
+    torch.cuda.synchronize()
+    launches = F.launch_count() - launches0
     with ClockSampler(torch.cuda.current_device()) as clk:
-        ms_graph = timed(lambda: b.replay(stream), args.steps, args.warmup)
-    launches = (F.launch_count() - launches0) // (args.steps + args.warmup)
-    ms_launch = timed(lambda: b.decompress(stream), args.steps, args.warmup)
-    ms_each = timed(lambda: b.decompress_each(False, stream), max(2, args.steps // 4), 2)
-    ms_each_sync = timed(lambda: b.decompress_each(True, stream), 2, 1)
+        ms_graph, n_graph = timed_loop(lambda: b.replay(stream), stream, args.steps, args.warmup)
+        ms_launch, _ = timed_loop(lambda: b.decompress(stream), stream, args.steps, args.warmup,
+                                  min_seconds=0.5)
+        ms_each, _ = timed_loop(lambda: b.decompress_each(False, stream), stream,
+                                max(2, args.steps // 4), 2, min_seconds=0.5)
+    ms_each_sync, _ = timed_loop(lambda: b.decompress_each(True, stream), stream, 2, 1,
+                                 min_seconds=0.0)
+    # full-size parity: the batched decode equals one flsgpu_decompress_*
+    # per column, bit for bit (checksums of every column's output)
+    for o in outs:
+        o.fill_(0)
+    b.replay(stream)
+    cs_batch = checksums()
+    for o in outs:
+        o.fill_(0)
+    b.decompress_each(False, stream)
+    cs_each = checksums()
+    batch_exact = bool(torch.equal(cs_batch, cs_each))
     q = F.PairQuery([p[0] for p in pairs], [p[1] for p in pairs], dev)
     q.capture(stream)
-    ms_query = timed(lambda: q.replay(stream), max(3, args.steps // 2), 3)
+    with ClockSampler(torch.cuda.current_device()) as qclk:
+        ms_query, _ = timed_loop(lambda: q.replay(stream), stream, max(3, args.steps // 2), 3,
+                                 min_seconds=1.0)
     q_read = sum(a.compressed_bytes() + bb.compressed_bytes() for a, bb in pairs)
-    return dict(ms=ms_graph, ms_launch=ms_launch, ms_each=ms_each, ms_each_sync=ms_each_sync,
-                read=read_b, write=write_b, clocks=clk.summary(), launches=launches,
-                n_values=sum(c.n_values for c in cols), gen_s=gen_s, ms_query=ms_query,
-                q_read=q_read, n_pairs=len(pairs))
+    del q, b
+    return dict(ms=ms_graph, steps=n_graph, ms_launch=ms_launch, ms_each=ms_each,
+                ms_each_sync=ms_each_sync, read=read_b, write=write_b, clocks=clk.summary(),
+                launches=launches, n_values=sum(c.n_values for c in cols), gen_s=gen_s,
+                ms_query=ms_query, q_read=q_read, n_pairs=len(pairs), q_clocks=qclk.summary(),
+                exact_vs_per_column=batch_exact, n_columns=len(cols))
 
 
 # ---------------------------------------------------------------------------
@@ -734,27 +845,20 @@ def run_learned(args, dev):
     l0, l1 = enc.train(train, epochs=args.epochs, batch=1024, lr=3e-3)
     train_s = time.perf_counter() - t0
 
-    def ev_time(fn, reps=3):
-        fn()
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(reps):
-            fn()
-        e1.record(stream)
-        torch.cuda.synchronize()
-        return e0.elapsed_time(e1) / reps
+    def ev_time(fn, min_seconds=0.5):
+        return timed_loop(fn, stream, 3, 1, min_seconds=min_seconds)[0]
 
     res = {}
-    ms_plain = ev_time(lambda: res.__setitem__("plain", enc.encode(evals, 0)))
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        ms_plain = ev_time(lambda: res.__setitem__("plain", enc.encode(evals, 0)))
+        ms_learned = ev_time(lambda: res.__setitem__("learned", enc.encode(evals, 1)))
     plain = res["plain"]
     plain_bytes = plain.compressed_bytes
-    ms_learned = ev_time(lambda: res.__setitem__("learned", enc.encode(evals, 1)))
     learned = res["learned"]
     col = F.encoded_column(learned, evals.numel(), enc)
     dec = F.decompress(col)
     exact = bool(torch.equal(dec.view(torch.int64), evals.view(torch.int64)))
+    del dec, col
     ms_search = ev_time(lambda: F.plain_labels(evals))
     ms_propose = ev_time(lambda: enc.propose(evals, 3))
     in_bytes = evals.numel() * 8
@@ -771,7 +875,7 @@ def run_learned(args, dev):
                 ms_propose=ms_propose, in_bytes=in_bytes, plain_bytes=plain_bytes,
                 learned_bytes=learned.compressed_bytes, fallback=int(learned.n_fallback),
                 n_rd=int(learned.n_rd), n_vecs=evals.numel() // 1024, exact=exact,
-                loss=(l0, l1), train_s=train_s,
+                loss=(l0, l1), train_s=train_s, clocks=clk.summary(),
                 ref_gbs=sample.nbytes / ref_s / 1e9 if ref_col is not None else None,
                 ref_ratio=sample.nbytes / ref_col["compressed_bytes"] if ref_col is not None else None)
 
@@ -829,6 +933,11 @@ def run_e2e(args, dev):
     return {"value": round((reads + writes) / (ms / 1e3) / 1e9, 2), "unit": "GB/s",
             "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
             "ms_per_step": round(ms, 3),
+            "share_of_headline": {"columns": "8 of the headline's 98 (u32 w 1, 7, 16, 32; u64 w 1, "
+                                             "20, 40, 64), a quarter of their values each",
+                                  "bytes_fraction": round((reads + writes) / HEADLINE_STEP_BYTES, 4),
+                                  "bound": "PCIe: every step moves the compressed column in and the "
+                                           "decoded values out"},
             "sample": "u32 2^26 values x w{1,7,16,32} + u64 2^25 x w{1,20,40,64}, pinned host "
                       "buffers, flsgpu_host_decompress_ffor_*_async for the 8 columns then "
                       "flsgpu_host_pipeline_sync (chunks of 2^22 values, copies overlapping the "
@@ -910,6 +1019,9 @@ def main():
                     help="fraction of the benchmark column sizes (1.0 = full)")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-extras", dest="extras", action="store_false",
+                    help="ffor workload: only the headline FFOR decode (no fused-sum, ALP, "
+                         "batch and learned blocks)")
     ap.add_argument("--only", default="",
                     help="ffor workload: columns to build, e.g. u32:6,u64:20 (profiling)")
     args = ap.parse_args()
@@ -950,41 +1062,6 @@ def main():
     import torch
     rank, world, local = dist_init()
     dev = torch.device("cuda", torch.cuda.current_device())
-    if args.workload == "learned":
-        r = run_learned(args, dev)
-        gbs_l = r["in_bytes"] / (r["ms_learned"] / 1e3) / 1e9
-        gbs_p = r["in_bytes"] / (r["ms_plain"] / 1e3) / 1e9
-        if rank == 0:
-            print(json.dumps({
-                "metric": "ALP encode GB/s (input bytes / end-to-end GPU encode), learned vs plain",
-                "value": round(gbs_l, 1), "unit": "GB/s", "n_gpus": world, "steps": 3,
-                "warmup": 1, "ms_per_step": round(r["ms_learned"], 3), "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": "learned ALP parameter proposal: f64 column of "
-                                       f"{r['n_vecs'] * 1024} values (d in 0..6, scale 10^0..8, "
-                                       "Gaussian/uniform, 10% noise vectors); network trained "
-                                       "on a separate 2^24-value column"},
-                "learned": {"encode_gbs": round(gbs_l, 1), "ms": round(r["ms_learned"], 3),
-                            "ratio": round(r["in_bytes"] / r["learned_bytes"], 4),
-                            "fallback_vectors": r["fallback"], "rd_vectors": r["n_rd"],
-                            "proposal_ms": round(r["ms_propose"], 3),
-                            "decode_bit_exact": r["exact"]},
-                "plain": {"encode_gbs": round(gbs_p, 1), "ms": round(r["ms_plain"], 3),
-                          "ratio": round(r["in_bytes"] / r["plain_bytes"], 4),
-                          "search_ms": round(r["ms_search"], 3)},
-                "speedup_encode_vs_plain": round(r["ms_plain"] / r["ms_learned"], 2),
-                "speedup_selection_vs_plain_search": round(r["ms_search"] / r["ms_propose"], 2),
-                "ratio_loss_vs_plain": round(1 - r["plain_bytes"] / r["learned_bytes"], 4),
-                "training": {"epochs": args.epochs, "seconds": round(r["train_s"], 2),
-                             "loss_first_epoch": round(r["loss"][0], 4),
-                             "loss_last_epoch": round(r["loss"][1], 4)},
-                "cpu_baseline": {"value": round(r["ref_gbs"], 3) if r["ref_gbs"] else None,
-                                 "unit": "GB/s", "cores": 1, "kind": "port",
-                                 "ratio": round(r["ref_ratio"], 4) if r["ref_ratio"] else None,
-                                 "sample": "the whole evaluation column, oracle restatement of "
-                                           "alp::encode with rowgroup sampling (100 vectors per "
-                                           "state, ALP-RD rowgroups kept on ALP)"}}))
-        return
     if args.tune or args.workload == "autotune":
         import flsgpu_b200 as F
         t0 = time.perf_counter()
@@ -1002,79 +1079,50 @@ def main():
                     "report": tuned["report"],
                     "header": F.tuning_header(tab)}))
             return
-    if args.workload == "alp":
-        r = run_alp(args, rank, world, dev)
-        pk, pk_kind = peaks()
-        hbm = float(pk["hbm_gbs"])
+    if args.workload == "learned":
         if rank == 0:
-            print(json.dumps({
-                "metric": "ALP / ALP-RD decode GB/s (compressed read + decoded write), 1 B200",
-                "value": round(r["gbs"], 1), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": round(r["ms"] / args.steps, 3),
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "f64/f32", "data": "synthetic",
-                "config": {"workload": "ALP/ALP-RD decode: f64 ALP 2^27 values (d 0..4, 1% "
-                                       "exceptions), f64 ALP-RD 2^27 uniform [0,1), f32 ALP 2^28 "
-                                       "values (d 0..3, 1% exceptions)",
-                           "scale": args.scale,
-                           "l2": "every column's output (1 GiB) exceeds L2; no flush",
-                           "parallelism": f"replicas x{args.gpus}"},
-                "per_column": r["per"], "bit_exact": r["exact"],
-                "hbm_fraction": {f"of_{pk_kind}": round(r["gbs"] / world / hbm, 4),
-                                 "of_spec_8tbs": round(r["gbs"] / world / 8000.0, 4)},
-                "roofline": {"bound": "hbm", "achieved": round(r["achieved"], 1), "peak": hbm,
-                             "unit": "GB/s", "frac": round(r["achieved"] / hbm, 4),
-                             "peak_kind": pk_kind,
-                             "kernel": "k_store<f64/f32, ALP> and k_alprd<f64>",
-                             "algorithmic_bytes_per_launch": round(r["bytes_step"] / 3),
-                             "traffic": profiled_traffic("alp_decode_at_scale.md",
-                                                         r["bytes_step"] / 3),
-                             "traffic_source": "profiles/alp_decode_at_scale.md (ncu, one pass)"},
-                "cpu_baseline": r["cpu"],
-                "gpu_launches": r["launches"], "clocks": r["clocks"],
-                "generation_s": round(r["gen_s"], 1)}))
+            print(json.dumps(learned_block(args, dev, world)))
+        return
+    if args.workload == "alp":
+        b = alp_block(args, rank, world, dev)
+        if rank == 0:
+            print(json.dumps(b))
         return
     if args.workload == "batch":
-        r = run_batch(args, dev)
-        pk, pk_kind = peaks()
-        hbm = float(pk["hbm_gbs"])
-        gbs = (r["read"] + r["write"]) / (r["ms"] / 1e3) / 1e9
+        b = batch_block(args, dev, world)
         if rank == 0:
-            print(json.dumps({
-                "metric": "batched uneven decode GB/s (compressed read + decoded write), 1 B200",
-                "value": round(gbs, 1), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": round(r["ms"], 3), "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "u32/f32/f64", "data": "synthetic",
-                "config": {"workload": f"batched uneven decode: {args.columns} columns, lengths "
-                                       "log-uniform 2^10..2^24 (x1024), types f64 ALP / u32 FFOR / "
-                                       "f32 ALP, one persistent launch replayed from a CUDA graph",
-                           "values": r["n_values"], "compressed_bytes": r["read"],
-                           "decoded_bytes": r["write"],
-                           "l2": "total decoded bytes exceed L2; no flush"},
-                "hbm_fraction": {f"of_{pk_kind}": round(gbs / hbm, 4), "of_spec_8tbs": round(gbs / 8000, 4)},
-                "per_column_launches_ms": round(r["ms_each"], 3),
-                "per_column_launches_sync_ms": round(r["ms_each_sync"], 3),
-                "eager_single_launch_ms": round(r["ms_launch"], 3),
-                "speedup_vs_per_column": round(r["ms_each"] / r["ms"], 2),
-                "speedup_vs_per_column_sync": round(r["ms_each_sync"] / r["ms"], 2),
-                "pair_query": {"pairs": r["n_pairs"], "ms": round(r["ms_query"], 3),
-                               "compressed_gbs": round(r["q_read"] / (r["ms_query"] / 1e3) / 1e9, 1),
-                               "what": "sum(A where B < median(B)) per (f64 ALP, u32 FFOR) pair, "
-                                       "4 radix passes over packed B + 1 fused decode/sum pass"},
-                "roofline": {"bound": "hbm", "achieved": round(gbs, 1), "peak": hbm, "unit": "GB/s",
-                             "frac": round(gbs / hbm, 4), "peak_kind": pk_kind,
-                             "kernel": "k_batch (flsgpu_batch_replay)", "traffic": None},
-                "gpu_launches": r["launches"], "clocks": r["clocks"],
-                "generation_s": round(r["gen_s"], 1)}))
+            print(json.dumps(b))
         return
     res = run_ffor(args, rank, world, dev)
+    torch.cuda.empty_cache()
     e2e = None if args.no_e2e else run_e2e(args, dev)
     pk, pk_kind = peaks()
     hbm = float(pk["hbm_gbs"])
+    extras = {}
+    if args.extras and args.workload == "ffor":
+        # the rest of the benchmark metric, each block with its own clocks:
+        # fused sum (same columns), ALP / ALP-RD decode, batched decode + pair
+        # query, learned vs plain ALP encode
+        extras["ffor_sum"] = res["fsum"]
+        torch.cuda.empty_cache()
+        extras["alp_decode"] = alp_block(args, rank, world, dev)
+        torch.cuda.empty_cache()
+        extras["batch_decode"] = batch_block(args, dev, world)
+        torch.cuda.empty_cache()
+        extras["learned_encode"] = learned_block(args, dev, world)
     if rank == 0:
-        cpu = cpu_reference_ffor(args.cpu_seconds) if world == 1 else None
+        cpu = None
+        if world == 1:
+            cpu = cpu_reference_ffor(args.cpu_seconds)
+            one = cpu_reference_ffor(args.cpu_seconds / 2, threads=1)
+            cpu["nproc"] = os.cpu_count()
+            cpu["single_thread"] = {"value": one["value"], "unit": "GB/s", "cores": 1,
+                                    "sample": one["sample"]}
+        name = "FFOR decode GB/s (compressed read + decoded write), 1 B200"
+        if args.workload == "ffor-sum":
+            name = "FFOR decode fused with a sum GB/s (compressed read + 8 B per column), 1 B200"
         line = {
-            "metric": metric, "value": round(res["gbs"], 1), "unit": "GB/s",
+            "metric": name, "value": round(res["gbs"], 1), "unit": "GB/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(res["ms"] / args.steps, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32/u64", "data": "synthetic",
@@ -1094,10 +1142,123 @@ def main():
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": res["launches"],
             "clocks": res["clocks"],
         }
+        line.update(extras)
         print(json.dumps(line))
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def alp_block(args, rank, world, dev) -> dict:
+    """The ALP / ALP-RD decode configuration: per column GB/s, fraction of
+    the HBM peak and a bit-exact flag, the f64 column again in the extended
+    layout, the reference's CPU decoder beside it."""
+    r = run_alp(args, rank, world, dev)
+    pk, pk_kind = peaks()
+    hbm = float(pk["hbm_gbs"])
+    return {
+        "metric": "ALP / ALP-RD decode GB/s (compressed read + decoded write), 1 B200",
+        "value": round(r["gbs"], 1), "unit": "GB/s", "n_gpus": world, "steps": r["steps"],
+        "warmup": args.warmup, "ms_per_step": round(r["ms"] / r["steps"], 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64/f32", "data": "synthetic",
+        "config": {"workload": "ALP/ALP-RD decode: f64 ALP 2^27 values (d 0..4, 1% "
+                               "exceptions), f64 ALP-RD 2^27 uniform [0,1), f32 ALP 2^28 "
+                               "values (d 0..3, 1% exceptions)",
+                   "scale": args.scale,
+                   "l2": "every column's output (1 GiB) exceeds L2; no flush",
+                   "parallelism": f"replicas x{world}"},
+        "per_column": r["per"], "bit_exact": r["exact"],
+        "hbm_fraction": {f"of_{pk_kind}": round(r["gbs"] / world / hbm, 4),
+                         "of_spec_8tbs": round(r["gbs"] / world / 8000.0, 4)},
+        "roofline": {"bound": "hbm", "achieved": round(r["achieved"], 1), "peak": hbm,
+                     "unit": "GB/s", "frac": round(r["achieved"] / hbm, 4),
+                     "peak_kind": pk_kind,
+                     "kernel": "k_store<f64/f32, ALP> and k_alprd<f64>",
+                     "algorithmic_bytes_per_launch": round(r["bytes_step"] / 3),
+                     "traffic": profiled_traffic("alp_decode_at_scale.md", r["bytes_step"] / 3),
+                     "traffic_source": "profiles/alp_decode_at_scale.md (ncu, one pass)"},
+        "cpu_baseline": r["cpu"],
+        "gpu_launches": r["launches"], "clocks": r["clocks"],
+        "generation_s": round(r["gen_s"], 1)}
+
+
+def batch_block(args, dev, world) -> dict:
+    """Batched uneven decode (graph replay) against one launch per column,
+    plus the fused pair query."""
+    r = run_batch(args, dev)
+    pk, pk_kind = peaks()
+    hbm = float(pk["hbm_gbs"])
+    gbs = (r["read"] + r["write"]) / (r["ms"] / 1e3) / 1e9
+    return {
+        "metric": "batched uneven decode GB/s (compressed read + decoded write), 1 B200",
+        "value": round(gbs, 1), "unit": "GB/s", "n_gpus": world, "steps": r["steps"],
+        "warmup": args.warmup, "ms_per_step": round(r["ms"], 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32/f32/f64", "data": "synthetic",
+        "config": {"workload": f"batched uneven decode: {r['n_columns']} columns, lengths "
+                               "log-uniform 2^10..2^24 (x1024), types f64 ALP / u32 FFOR / "
+                               "f32 ALP, persistent launches replayed from a CUDA graph",
+                   "values": r["n_values"], "compressed_bytes": r["read"],
+                   "decoded_bytes": r["write"],
+                   "l2": "total decoded bytes exceed L2; no flush"},
+        "hbm_fraction": {f"of_{pk_kind}": round(gbs / hbm, 4), "of_spec_8tbs": round(gbs / 8000, 4)},
+        "bit_exact_vs_per_column": r["exact_vs_per_column"],
+        "per_column_launches_ms": round(r["ms_each"], 3),
+        "per_column_launches_sync_ms": round(r["ms_each_sync"], 3),
+        "eager_batch_launch_ms": round(r["ms_launch"], 3),
+        "speedup_vs_per_column": round(r["ms_each"] / r["ms"], 2),
+        "speedup_vs_per_column_sync": round(r["ms_each_sync"] / r["ms"], 2),
+        "pair_query": {"pairs": r["n_pairs"], "ms": round(r["ms_query"], 3),
+                       "compressed_gbs": round(r["q_read"] / (r["ms_query"] / 1e3) / 1e9, 1),
+                       "what": "sum(A where B < median(B)) per (f64 ALP, u32 FFOR) pair, "
+                               "4 radix passes over packed B + 1 fused decode/sum pass",
+                       "clocks": r["q_clocks"]},
+        "roofline": {"bound": "hbm", "achieved": round(gbs, 1), "peak": hbm, "unit": "GB/s",
+                     "frac": round(gbs / hbm, 4), "peak_kind": pk_kind,
+                     "kernel": "k_batch (flsgpu_batch_replay)",
+                     "traffic": profiled_traffic("batch_decode_launches.md", r["read"] + r["write"]),
+                     "traffic_source": "profiles/batch_decode_launches.md"},
+        "gpu_launches_per_replay": r["launches"], "clocks": r["clocks"],
+        "generation_s": round(r["gen_s"], 1)}
+
+
+def learned_block(args, dev, world) -> dict:
+    """Learned ALP parameter proposal against the plain per-vector search:
+    end-to-end GPU encode GB/s, compression ratio, fallbacks, selection and
+    end-to-end speed-ups, bit-exact decode."""
+    r = run_learned(args, dev)
+    gbs_l = r["in_bytes"] / (r["ms_learned"] / 1e3) / 1e9
+    gbs_p = r["in_bytes"] / (r["ms_plain"] / 1e3) / 1e9
+    return {
+        "metric": "ALP encode GB/s (input bytes / end-to-end GPU encode), learned vs plain",
+        "value": round(gbs_l, 1), "unit": "GB/s", "n_gpus": world,
+        "ms_per_step": round(r["ms_learned"], 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "learned ALP parameter proposal: f64 column of "
+                               f"{r['n_vecs'] * 1024} values (d in 0..6, scale 10^0..8, "
+                               "Gaussian/uniform, 10% noise vectors); network trained "
+                               "on a separate 2^24-value column"},
+        "learned": {"encode_gbs": round(gbs_l, 1), "ms": round(r["ms_learned"], 3),
+                    "ratio": round(r["in_bytes"] / r["learned_bytes"], 4),
+                    "fallback_vectors": r["fallback"], "rd_vectors": r["n_rd"],
+                    "proposal_ms": round(r["ms_propose"], 3),
+                    "decode_bit_exact": r["exact"]},
+        "plain": {"encode_gbs": round(gbs_p, 1), "ms": round(r["ms_plain"], 3),
+                  "ratio": round(r["in_bytes"] / r["plain_bytes"], 4),
+                  "search_ms": round(r["ms_search"], 3)},
+        "speedup_encode_vs_plain": round(r["ms_plain"] / r["ms_learned"], 2),
+        "speedup_selection_vs_plain_search": round(r["ms_search"] / r["ms_propose"], 2),
+        "ratio_loss_vs_plain": round(1 - r["plain_bytes"] / r["learned_bytes"], 4),
+        "training": {"epochs": args.epochs, "seconds": round(r["train_s"], 2),
+                     "loss_first_epoch": round(r["loss"][0], 4),
+                     "loss_last_epoch": round(r["loss"][1], 4)},
+        "clocks": r["clocks"],
+        "cpu_baseline": {"value": round(r["ref_gbs"], 3) if r["ref_gbs"] else None,
+                         "unit": "GB/s", "cores": 1, "kind": "port",
+                         "ratio": round(r["ref_ratio"], 4) if r["ref_ratio"] else None,
+                         "sample": "the whole evaluation column, oracle restatement of "
+                                   "alp::encode with rowgroup sampling (100 vectors per "
+                                   "state, ALP-RD rowgroups kept on ALP)"}}
 
 
 if __name__ == "__main__":

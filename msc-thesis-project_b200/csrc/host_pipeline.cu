@@ -47,6 +47,18 @@ static flsgpu_status stage_ffor(flsgpu_host_pipeline *p, int sl, const flsgpu_ff
   const size_t w1 = hc->bp.vector_offsets[v1 - 1] + (size_t)hc->bp.bit_widths[v1 - 1] * NL;
   if (w1 < w0 || w1 - w0 > p->chunk_vecs * 1024)
     return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "host column: vector offsets out of order");
+  // every vector's packed words must lie inside the staged range [w0, w1):
+  // the decode addresses them through a base moved back by w0.  Widths
+  // beyond the type are left to the kernel's metadata check (it skips the
+  // vector and raises FLSGPU_BAD_BIT_WIDTH).
+  for (size_t v = v0; v < v1; ++v) {
+    const size_t bw = hc->bp.bit_widths[v], off = hc->bp.vector_offsets[v];
+    if (bw > sizeof(U) * 8) continue;
+    if (off < w0 || off > w1 || bw * NL > w1 - off)
+      return set_error(FLSGPU_ERR_INVALID_ARGUMENT,
+                       "host column: vector %zu packed words [%zu, +%zu) outside its chunk", v, off,
+                       bw * NL);
+  }
   unsigned char *m = p->d_meta[sl];
   size_t *d_offs = reinterpret_cast<size_t *>(m);
   U *d_bases = reinterpret_cast<U *>(m + 8 * nv);
@@ -86,6 +98,12 @@ static flsgpu_status stage_alp(flsgpu_host_pipeline *p, int sl, const flsgpu_alp
   const size_t e1 = hc->exceptions_offsets[v1 - 1] + hc->counts[v1 - 1];
   if (e1 < e0 || e1 - e0 > p->chunk_vecs * 1024)
     return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "host column: exception offsets out of order");
+  for (size_t v = v0; v < v1; ++v) {
+    const size_t eo = hc->exceptions_offsets[v], cnt = hc->counts[v];
+    if (eo < e0 || eo > e1 || cnt > e1 - eo)
+      return set_error(FLSGPU_ERR_INVALID_ARGUMENT,
+                       "host column: vector %zu exceptions [%zu, +%zu) outside its chunk", v, eo, cnt);
+  }
   unsigned char *ex = p->d_exc[sl];
   T *d_ex = reinterpret_cast<T *>(ex);
   uint16_t *d_pos = reinterpret_cast<uint16_t *>(ex + p->chunk_vecs * 1024 * sizeof(T));

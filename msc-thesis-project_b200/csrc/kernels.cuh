@@ -531,7 +531,14 @@ __global__ void __launch_bounds__(256, min_blocks<T, VAR>()) k_column(const Kern
       if (meta.w <= (int)(sizeof(U) * 8) && prefetch_width(p, meta.w))
         prefetch_packed(reinterpret_cast<const U *>(c.packed) + meta.off, meta.w, t);
     }
-    if (!setup_from_meta<T, KIND>(c, p.d_status, cur, t, vin, w, xf)) continue;
+    if (!setup_from_meta<T, KIND>(c, p.d_status, cur, t, vin, w, xf)) {
+      // a rejected vector (status flag raised) adds +0.0: its slot of the
+      // fixed tree gets a defined value, never what the buffer held before
+      if constexpr (STAGE && SINK == S_SUM) {
+        if (t == 0) p.partials[vi] = 0.0;
+      }
+      continue;
+    }
     const size_t vbase = vi * VEC;
     const size_t rem = c.n_values - vbase;
     const int lim = rem < (size_t)VEC ? (int)rem : VEC;

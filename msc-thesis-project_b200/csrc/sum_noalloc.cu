@@ -17,8 +17,17 @@
 // larger columns are rejected.  Every call on a device uses the same array,
 // so calls whose kernels overlap on the GPU (different streams, or several
 // host threads) race on it; serialise them.  Each call overwrites every
-// partial it reads, so stale contents from an earlier call never leak into
-// a result and nothing has to be cleared.
+// partial it reads (a vector rejected by the metadata checks writes +0.0),
+// so stale contents from an earlier call never leak into a result and
+// nothing has to be cleared.
+//
+// The device address is cached per device index for the life of the
+// process.  cudaDeviceReset (or anything else that destroys the primary
+// context) reloads the module and invalidates it, so the cache is keyed by
+// the context as well: a call made in a different context than the one
+// the address was taken in looks it up again.
+#include <cuda.h>
+
 #include <mutex>
 
 #include "kernels.cuh"
@@ -32,22 +41,33 @@ constexpr size_t kNoAllocScratch = kNoAllocMaxVectors + (kNoAllocMaxVectors + 20
 static __device__ __align__(256) double g_noalloc_partials[kNoAllocScratch];
 
 // In host code g_noalloc_partials names a host-side stand-in, not device
-// memory: its device address is looked up once per device, with that device
-// current, and cached.
+// memory: its device address is looked up with the device current, and
+// cached per device together with the id of the context it was taken in.
 static std::mutex g_noalloc_mu;
 static double *g_noalloc_addr[64] = {nullptr};
+static unsigned long long g_noalloc_ctx[64] = {0};
 
 static flsgpu_status noalloc_scratch(double **out) {
   int dev = 0;
   flsgpu_status s = check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
   if (s) return s;
   if (dev < 0 || dev >= 64) return set_error(FLSGPU_ERR_UNSUPPORTED, "device index %d", dev);
+  // the id of the context current on this thread (none yet when the CUDA
+  // runtime has not been used on it: then the lookup below binds the
+  // device's primary context and the id is read afterwards)
+  CUcontext ctx = nullptr;
+  unsigned long long ctx_id = 0;
+  if (cuCtxGetCurrent(&ctx) != CUDA_SUCCESS || !ctx || cuCtxGetId(ctx, &ctx_id) != CUDA_SUCCESS)
+    ctx_id = 0;
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_addr[dev]) {
+  if (!g_noalloc_addr[dev] || ctx_id == 0 || g_noalloc_ctx[dev] != ctx_id) {
     void *p = nullptr;
     s = check_cuda(cudaGetSymbolAddress(&p, g_noalloc_partials), "cudaGetSymbolAddress");
     if (s) return s;
+    if (cuCtxGetCurrent(&ctx) != CUDA_SUCCESS || !ctx || cuCtxGetId(ctx, &ctx_id) != CUDA_SUCCESS)
+      return set_error(FLSGPU_ERR_CUDA, "flsgpu_sum_alp_f64_noalloc: no current CUDA context");
     g_noalloc_addr[dev] = static_cast<double *>(p);
+    g_noalloc_ctx[dev] = ctx_id;
   }
   *out = g_noalloc_addr[dev];
   return FLSGPU_OK;

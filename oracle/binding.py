@@ -34,7 +34,13 @@ def build_oracle(force: bool = False) -> Path:
     return ORACLE_SO
 
 
-def build_ref(reference: str = "/root/reference") -> Path | None:
+def reference_root() -> str:
+    """The reference checkout: $FLSGPU_REFERENCE, default /root/reference."""
+    return os.environ.get("FLSGPU_REFERENCE", "/root/reference")
+
+
+def build_ref(reference: str | None = None) -> Path | None:
+    reference = reference or reference_root()
     if not Path(reference, "src", "fls").is_dir():
         return REF_SO if REF_SO.exists() else None
     subprocess.check_call(["bash", str(HERE / "build_ref.sh"), reference])

@@ -7,7 +7,7 @@
 # (src/alp/encoder.hpp:342-350 does not compile under AVX-512) and with
 # -ffp-contract=off (the ALP encoder's rounding trick must not become an FMA).
 set -euo pipefail
-REF="${1:-/root/reference}"
+REF="${1:-${FLSGPU_REFERENCE:-/root/reference}}"
 HERE="$(cd "$(dirname "$0")" && pwd)"
 OUT="$HERE/_ref"
 if [ ! -d "$REF/src/fls" ]; then

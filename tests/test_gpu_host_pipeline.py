@@ -83,3 +83,43 @@ def test_host_pipeline_async_series(cuda):
         ut = np.uint64 if bits == 64 else np.uint32
         want = B.decode_ffor(c["packed"], c["bit_widths"], c["vector_offsets"], c["bases"], bits)
         assert np.array_equal(out.numpy().view(ut), want[:n_values])
+
+
+def test_host_pipeline_rejects_offsets_outside_the_chunk(cuda):
+    """A vector in the middle of a chunk whose packed words (or exceptions)
+    lie outside the chunk's staged range is refused before any copy, with
+    FLSGPU_ERR_INVALID_ARGUMENT: the decode would otherwise read outside the
+    staging slot."""
+    import torch
+    n_vecs, bits = 6, 32
+    c = colgen.random_ffor(90, n_vecs, bits, [5, 9])
+    offs = c["vector_offsets"].copy()
+    offs[1] = offs[4] + 10_000  # second vector of the first chunk points far past it
+    t = [_pinned(c["packed"].view(np.int32)), _pinned(c["bit_widths"]),
+         _pinned(offs.view(np.int64)), _pinned(c["bases"].view(np.int32))]
+    desc, kind, dt, keep = F.host_ffor_column(*t, n_vecs * 1024)
+    out = torch.empty(n_vecs * 1024, dtype=torch.int32).pin_memory()
+    pipe = F.HostPipeline(chunk_values=3072)
+    with pytest.raises(F.FlsgpuError) as e:
+        pipe.decompress(desc, kind, dt, out)
+    assert e.value.status == 1 and "outside its chunk" in str(e.value)
+
+    col = colgen.random_alp(91, n_vecs, True, [8], [4])
+    col["exceptions_offsets"] = col["exceptions_offsets"].copy()
+    col["exceptions_offsets"][1] = 10_000
+    signed = {np.dtype(np.uint64): np.int64, np.dtype(np.uint32): np.int32,
+              np.dtype(np.uint16): np.int16}
+    keep = {k: _pinned(v.view(signed[v.dtype]) if v.dtype in signed else v)
+            for k, v in col.items() if isinstance(v, np.ndarray)}
+    n_values = n_vecs * 1024
+    bp = F.BPColumnC(n_values, n_vecs, keep["packed"].data_ptr(), keep["bit_widths"].data_ptr(),
+                     keep["vector_offsets"].data_ptr())
+    ac = F.ALPColumnC(n_values, F.FFORColumnC(n_values, bp, keep["bases"].data_ptr()), None, None,
+                      keep["factor_indices"].data_ptr(), keep["fraction_indices"].data_ptr(),
+                      int(keep["exceptions"].numel()), keep["exceptions_offsets"].data_ptr(),
+                      keep["exceptions"].data_ptr(), keep["positions"].data_ptr(),
+                      keep["counts"].data_ptr())
+    outf = torch.empty(n_values, dtype=torch.float64).pin_memory()
+    with pytest.raises(F.FlsgpuError) as e:
+        F.HostPipeline(chunk_values=3072).decompress(ac, "alp", "f64", outf)
+    assert e.value.status == 1 and "outside its chunk" in str(e.value)
