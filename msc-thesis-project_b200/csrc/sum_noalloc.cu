@@ -47,24 +47,50 @@ static std::mutex g_noalloc_mu;
 static double *g_noalloc_addr[64] = {nullptr};
 static unsigned long long g_noalloc_ctx[64] = {0};
 
+// Process-unique id of the context current on the calling thread, 0 when
+// there is none.  The two driver entry points are looked up through the
+// runtime, so the library does not link against the driver library itself
+// (it still loads where no GPU driver is installed).
+static unsigned long long current_context_id() {
+  using get_current_t = CUresult (*)(CUcontext *);
+  using get_id_t = CUresult (*)(CUcontext, unsigned long long *);
+  static get_current_t get_current = nullptr;
+  static get_id_t get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<get_current_t>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<get_id_t>(f);
+  });
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (!get_current || !get_id || get_current(&ctx) != CUDA_SUCCESS || !ctx ||
+      get_id(ctx, &id) != CUDA_SUCCESS)
+    return 0;
+  return id;
+}
+
 static flsgpu_status noalloc_scratch(double **out) {
   int dev = 0;
   flsgpu_status s = check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
   if (s) return s;
   if (dev < 0 || dev >= 64) return set_error(FLSGPU_ERR_UNSUPPORTED, "device index %d", dev);
-  // the id of the context current on this thread (none yet when the CUDA
-  // runtime has not been used on it: then the lookup below binds the
-  // device's primary context and the id is read afterwards)
-  CUcontext ctx = nullptr;
-  unsigned long long ctx_id = 0;
-  if (cuCtxGetCurrent(&ctx) != CUDA_SUCCESS || !ctx || cuCtxGetId(ctx, &ctx_id) != CUDA_SUCCESS)
-    ctx_id = 0;
+  // the id of the context current on this thread (0 when the CUDA runtime
+  // has not been used on it yet: then the lookup below binds the device's
+  // primary context and the id is read afterwards)
+  unsigned long long ctx_id = current_context_id();
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
   if (!g_noalloc_addr[dev] || ctx_id == 0 || g_noalloc_ctx[dev] != ctx_id) {
     void *p = nullptr;
     s = check_cuda(cudaGetSymbolAddress(&p, g_noalloc_partials), "cudaGetSymbolAddress");
     if (s) return s;
-    if (cuCtxGetCurrent(&ctx) != CUDA_SUCCESS || !ctx || cuCtxGetId(ctx, &ctx_id) != CUDA_SUCCESS)
+    if ((ctx_id = current_context_id()) == 0)
       return set_error(FLSGPU_ERR_CUDA, "flsgpu_sum_alp_f64_noalloc: no current CUDA context");
     g_noalloc_addr[dev] = static_cast<double *>(p);
     g_noalloc_ctx[dev] = ctx_id;
