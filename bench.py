@@ -382,10 +382,9 @@ def make_alp_columns(scale: float, dev, seed: int = 31):
       10^d (d uniform per vector in 0..4), 1% of positions replaced by random
       non-NaN 64-bit patterns; encoded by the library's GPU encoder (plain
       per-vector search);
-    * f64 ALP-RD, 2^27 values uniform in [0, 1) with full mantissa: cut at
-      52 bits (right part = mantissa, left part = exponent), dictionary of the
-      8 most frequent exponents, other exponents as exceptions, both parts
-      packed by the GPU packer (BP);
+    * f64 ALP-RD, 2^27 values uniform in [0, 1) with full mantissa, encoded
+      by the library's GPU ALP-RD encoder (cut and dictionary per rowgroup of
+      100 vectors);
     * f32 ALP, 2^28 values: integers uniform in [-10^6, 10^6] times
       FRAC[d] (d uniform per vector in 0..3, factor 0: the value ALP decodes
       them to), FFOR-packed at the signed minimum by the GPU packer, 1% of
@@ -423,36 +422,15 @@ def make_alp_columns(scale: float, dev, seed: int = 31):
     rd_b = int(res.n_packed_words) * 8 + nv * 29 + int(res.n_exceptions) * 10
     out.append(("alp_f64", col, vals, rd_b, n * 8))
 
-    # f64 ALP-RD
+    # f64 ALP-RD, encoded by the library's GPU ALP-RD encoder: one cut and
+    # dictionary per rowgroup of 100 vectors (rd_encoder::init / encode)
     vals = torch.rand(n, dtype=torch.float64, device=dev, generator=g)
-    bits = vals.view(torch.int64)
-    left = bits >> 52
-    right = bits & ((1 << 52) - 1)
-    cnt = torch.bincount(left, minlength=2048)
-    top = torch.argsort(cnt, descending=True, stable=True)[:8]
-    lut = torch.full((2048,), -1, dtype=torch.int64, device=dev)
-    lut[top] = torch.arange(8, device=dev)
-    idx = lut[left]
-    mask = idx < 0
-    counts, eoffs, flat, pos = exc_layout(mask, nv)
-    exc = left[flat].to(torch.int16)
-    rcol = F.ffor_encode(right, F.BASE_ZERO)
-    assert int(rcol.buffers["bit_widths"].min()) == 52 and int(rcol.buffers["bit_widths"].max()) == 52
-    lbuf = F.ffor_encode(idx.clamp(min=0).to(torch.int16), F.BASE_ZERO)
-    dicts = top.to(torch.int16)
-    dict_idx = torch.zeros(nv, dtype=torch.int32, device=dev)
-    left_c = F.BPColumnC(n, nv, lbuf["_keep"].data_ptr(), lbuf["bit_widths"].data_ptr(),
-                         lbuf["vector_offsets"].data_ptr())
-    n_exc = int(flat.numel())
-    c = F.ALPRDColumnC(n, rcol.c, left_c, dicts.data_ptr(), dict_idx.data_ptr(), n_exc,
-                       eoffs.data_ptr(), exc.data_ptr() if n_exc else 0,
-                       pos.data_ptr() if n_exc else 0, counts.data_ptr())
-    keep = {"right": rcol, "left": lbuf, "dicts": dicts, "dict_idx": dict_idx, "exc": exc,
-            "pos": pos, "counts": counts, "eoffs": eoffs}
-    col = F.DeviceColumn("alprd", "f64", n, c, {"_keep": keep}, rcol.n_packed)
-    rd_b = rcol.n_packed * 8 + lbuf["n_packed"] * 2 + nv * 32 + 16 + n_exc * 4
+    rres = enc.encode_rd(vals, rowgroup_vecs=100)
+    col = F.rd_encoded_column(rres, n, "f64", enc)
+    nv = n // 1024
+    rd_b = (int(rres.n_right_words) * 8 + int(rres.n_left_words) * 2 + nv * 32
+            + int(rres.n_dictionaries) * 16 + int(rres.n_exceptions) * 4)
     out.append(("alprd_f64", col, vals, rd_b, n * 8))
-    del bits, left, right, idx, mask, lut
 
     # f32 ALP, compressed level with the values ALP decodes to
     n = int(2 ** 28 * scale) // 1024 * 1024
@@ -850,15 +828,23 @@ def run_learned(args, dev):
 
     res = {}
     with ClockSampler(torch.cuda.current_device()) as clk:
-        ms_plain = ev_time(lambda: res.__setitem__("plain", enc.encode(evals, 0)))
-        ms_learned = ev_time(lambda: res.__setitem__("learned", enc.encode(evals, 1)))
-    plain = res["plain"]
-    plain_bytes = plain.compressed_bytes
-    learned = res["learned"]
-    col = F.encoded_column(learned, evals.numel(), enc)
-    dec = F.decompress(col)
-    exact = bool(torch.equal(dec.view(torch.int64), evals.view(torch.int64)))
-    del dec, col
+        # hybrid columns: vectors that call for ALP-RD are encoded as ALP-RD
+        ms_plain = ev_time(lambda: res.__setitem__("plain", enc.encode_hybrid(evals, 0)))
+        plain = res["plain"]
+        plain_bytes, plain_rd = plain.compressed_bytes, int(plain.n_rd_vectors)
+        dec = F.decompress(F.hybrid_column(plain, evals.numel(), enc))
+        exact_plain = bool(torch.equal(dec.view(torch.int64), evals.view(torch.int64)))
+        ms_learned = ev_time(lambda: res.__setitem__("learned", enc.encode_hybrid(evals, 1)))
+        learned = res["learned"]
+        dec = F.decompress(F.hybrid_column(learned, evals.numel(), enc))
+        exact = bool(torch.equal(dec.view(torch.int64), evals.view(torch.int64))) and exact_plain
+        # the same two encoders writing ALP-only columns (ALP-RD vectors kept
+        # on their best ALP pair), as the reference's ALPColumn requires
+        ms_plain_a = ev_time(lambda: res.__setitem__("plain_a", enc.encode(evals, 0)))
+        ms_learned_a = ev_time(lambda: res.__setitem__("learned_a", enc.encode(evals, 1)))
+        dec = F.decompress(F.encoded_column(res["learned_a"], evals.numel(), enc))
+        exact = exact and bool(torch.equal(dec.view(torch.int64), evals.view(torch.int64)))
+    del dec
     ms_search = ev_time(lambda: F.plain_labels(evals))
     ms_propose = ev_time(lambda: enc.propose(evals, 3))
     in_bytes = evals.numel() * 8
@@ -871,10 +857,16 @@ def run_learned(args, dev):
     t = time.perf_counter()
     ref_col = B.alp_encode(sample, rowgroup_vecs=100, rd_as_alp=True)
     ref_s = time.perf_counter() - t
+    alp_only = {"plain_ms": round(ms_plain_a, 3), "learned_ms": round(ms_learned_a, 3),
+                "plain_ratio": round(in_bytes / res["plain_a"].compressed_bytes, 4),
+                "learned_ratio": round(in_bytes / res["learned_a"].compressed_bytes, 4),
+                "speedup": round(ms_plain_a / ms_learned_a, 2),
+                "fallback_vectors": int(res["learned_a"].n_fallback)}
     return dict(ms_plain=ms_plain, ms_learned=ms_learned, ms_search=ms_search,
                 ms_propose=ms_propose, in_bytes=in_bytes, plain_bytes=plain_bytes,
                 learned_bytes=learned.compressed_bytes, fallback=int(learned.n_fallback),
-                n_rd=int(learned.n_rd), n_vecs=evals.numel() // 1024, exact=exact,
+                n_rd=int(learned.n_rd_vectors), plain_rd=plain_rd, alp_only=alp_only,
+                n_vecs=evals.numel() // 1024, exact=exact,
                 loss=(l0, l1), train_s=train_s, clocks=clk.summary(),
                 ref_gbs=sample.nbytes / ref_s / 1e9 if ref_col is not None else None,
                 ref_ratio=sample.nbytes / ref_col["compressed_bytes"] if ref_col is not None else None)
@@ -1238,6 +1230,7 @@ def learned_block(args, dev, world) -> dict:
                                f"{r['n_vecs'] * 1024} values (d in 0..6, scale 10^0..8, "
                                "Gaussian/uniform, 10% noise vectors); network trained "
                                "on a separate 2^24-value column"},
+        "column": "hybrid: ALP vectors + ALP-RD vectors (flsgpu_alp_encode_hybrid_f64)",
         "learned": {"encode_gbs": round(gbs_l, 1), "ms": round(r["ms_learned"], 3),
                     "ratio": round(r["in_bytes"] / r["learned_bytes"], 4),
                     "fallback_vectors": r["fallback"], "rd_vectors": r["n_rd"],
@@ -1245,7 +1238,8 @@ def learned_block(args, dev, world) -> dict:
                     "decode_bit_exact": r["exact"]},
         "plain": {"encode_gbs": round(gbs_p, 1), "ms": round(r["ms_plain"], 3),
                   "ratio": round(r["in_bytes"] / r["plain_bytes"], 4),
-                  "search_ms": round(r["ms_search"], 3)},
+                  "rd_vectors": r["plain_rd"], "search_ms": round(r["ms_search"], 3)},
+        "alp_only_columns": r["alp_only"],
         "speedup_encode_vs_plain": round(r["ms_plain"] / r["ms_learned"], 2),
         "speedup_selection_vs_plain_search": round(r["ms_search"] / r["ms_propose"], 2),
         "ratio_loss_vs_plain": round(1 - r["plain_bytes"] / r["learned_bytes"], 4),

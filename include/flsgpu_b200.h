@@ -158,6 +158,22 @@ typedef struct flsgpu_alprd_column {
   uint16_t *counts;
 } flsgpu_alprd_column;
 
+/* Hybrid ALP / ALP-RD column (no counterpart in the reference, whose
+ * alp::encode rejects data that calls for ALP-RD; upstream ALP picks the
+ * scheme per rowgroup, src/alp/encoder.hpp:208-211): vector v is decoded
+ * from `alp` when schemes[v] == FLSGPU_SCHEME_ALP and from `rd` when
+ * schemes[v] == FLSGPU_SCHEME_ALP_RD.  Both sub-columns index every vector;
+ * a vector's entry in the other sub-column is empty (width 0, no
+ * exceptions, no packed words). */
+#define FLSGPU_SCHEME_ALP 0u
+#define FLSGPU_SCHEME_ALP_RD 1u
+typedef struct flsgpu_alphybrid_column {
+  size_t n_values;
+  flsgpu_alp_column alp;
+  flsgpu_alprd_column rd;
+  uint8_t *schemes;                    /* per vector */
+} flsgpu_alphybrid_column;
+
 typedef struct flsgpu_decode_opts {
   uint32_t unpack_n_vectors;  /* reference UNPACK_N_VECTORS (1, 4): advisory */
   uint32_t unpack_n_values;   /* reference UNPACK_N_VALUES (1, 32): advisory */
@@ -201,6 +217,13 @@ flsgpu_status flsgpu_decompress_alprd_f32(const flsgpu_alprd_column *column, flo
                                           const flsgpu_decode_opts *opts, flsgpu_stream stream);
 flsgpu_status flsgpu_decompress_alprd_f64(const flsgpu_alprd_column *column, double *d_out,
                                           const flsgpu_decode_opts *opts, flsgpu_stream stream);
+
+flsgpu_status flsgpu_decompress_alphybrid_f32(const flsgpu_alphybrid_column *column,
+                                              float *d_out, const flsgpu_decode_opts *opts,
+                                              flsgpu_stream stream);
+flsgpu_status flsgpu_decompress_alphybrid_f64(const flsgpu_alphybrid_column *column,
+                                              double *d_out, const flsgpu_decode_opts *opts,
+                                              flsgpu_stream stream);
 
 /* ---- FastLanes packing, the encoder side (fls::ffor src/fls/ffor.cpp:
  *      29861, fls::pack src/fls/pack.cpp:29731, base / width rule of

@@ -203,6 +203,65 @@ flsgpu_status flsgpu_alp_encoder_gradients(flsgpu_alp_encoder *encoder, const vo
                                            float *h_loss, flsgpu_stream stream);
 flsgpu_status flsgpu_alp_encoder_save(const flsgpu_alp_encoder *encoder, const char *path);
 flsgpu_status flsgpu_alp_encoder_load(flsgpu_alp_encoder *encoder, const char *path);
+/* Hybrid encode: as flsgpu_alp_encode_f64, but the vectors that call for
+ * ALP-RD are encoded as ALP-RD (upstream ALP switches scheme there,
+ * src/alp/encoder.hpp:208-211, where the reference's alp::encode gives up)
+ * into a flsgpu_alphybrid_column: mode 0 when the plain search's best
+ * estimate reaches the ALP-RD limit (48 bits per value on the samples);
+ * mode 1 when the network's top class is ALP-RD and none of its proposed ALP
+ * pairs estimates below that limit on the samples, or when the plain search
+ * of a fallback vector reaches it.  An ALP-RD vector carries a dictionary
+ * of its own, built from its 32 samples with the cut search of
+ * rd_encoder::init.  Decodes with flsgpu_decompress_alphybrid_f64. */
+typedef struct flsgpu_alp_hybrid_encode_result {
+  flsgpu_alphybrid_column column;  /* device arrays in the encoder's workspace */
+  size_t n_alp_vectors, n_rd_vectors;
+  size_t n_packed_words, n_exceptions;                  /* ALP part */
+  size_t n_right_words, n_left_words, n_rd_exceptions;  /* ALP-RD part */
+  size_t compressed_bytes;   /* ALP vectors as alp::encode accounts them, plus
+                                the ALP-RD vectors (words, 4 B per exception,
+                                48 B of dictionary and metadata) and one
+                                scheme byte per vector */
+  size_t n_fallback;         /* vectors that fell back to the plain search */
+  double mean_bit_width;     /* over the ALP vectors */
+  const uint8_t *d_flags;    /* per vector (device): bit 0 the plain search
+                                ran as fallback, bit 1 encoded as ALP-RD */
+} flsgpu_alp_hybrid_encode_result;
+flsgpu_status flsgpu_alp_encode_hybrid_f64(flsgpu_alp_encoder *encoder, const double *d_values,
+                                           size_t n_values, uint32_t mode,
+                                           flsgpu_alp_hybrid_encode_result *out,
+                                           flsgpu_stream stream);
+
+/* ---- GPU ALP-RD encoder (rd_encoder::init / encode, src/alp/rd.hpp:
+ *      28-140; the reference encodes ALP-RD on the CPU only and has no GPU
+ *      ALP-RD format) ---------------------------------------------------------
+ * One dictionary per rowgroup of rowgroup_vecs vectors (1..100; 100 is the
+ * reference's ROWGROUP_SIZE, src/alp/config.hpp): the rowgroup's
+ * first-level sample (every 12th vector, 32 values at stride 32 of each,
+ * sampler.hpp:11-48) picks the cut (find_best_dictionary: right width 48..63
+ * for f64, 16..31 for f32) and the <= 8 most frequent left parts (ties: the
+ * smaller left part first); every vector is then split into right parts
+ * (FastLanes lanes, FFOR base 0), dictionary indices (u16 FastLanes lanes at
+ * width max(1, ceil(log2(dictionary size)))) and exceptions (left part +
+ * position).  The column's arrays live in the encoder's workspace until its
+ * next encode; it decodes with flsgpu_decompress_alprd_*.  n_values % 1024 ==
+ * 0.  Synchronises (the sizes are read back). */
+typedef struct flsgpu_alprd_encode_result {
+  flsgpu_alprd_column column;
+  size_t n_right_words;      /* right-part words, of the value's width */
+  size_t n_left_words;       /* u16 words of dictionary indices */
+  size_t n_exceptions;
+  size_t n_dictionaries;     /* one per rowgroup */
+  size_t compressed_bytes;   /* words + 4 B per exception + 16 B per dictionary
+                                + 32 B of per-vector metadata */
+} flsgpu_alprd_encode_result;
+flsgpu_status flsgpu_alprd_encode_f64(flsgpu_alp_encoder *encoder, const double *d_values,
+                                      size_t n_values, uint32_t rowgroup_vecs,
+                                      flsgpu_alprd_encode_result *out, flsgpu_stream stream);
+flsgpu_status flsgpu_alprd_encode_f32(flsgpu_alp_encoder *encoder, const float *d_values,
+                                      size_t n_values, uint32_t rowgroup_vecs,
+                                      flsgpu_alprd_encode_result *out, flsgpu_stream stream);
+
 /* C (fp32 / bf16, M x N, row stride ldc) = A (bf16 M x K) . B (bf16 N x K)^T
  * [+ bias][relu] on the tensor cores (tcgen05, accumulator in TMEM);
  * N <= 256, K % 16 == 0, operands 16-byte aligned. */

@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "alp_learn.cuh"
+#include "rd_encode.cuh"
 
 namespace flsb200 {
 
@@ -32,6 +33,10 @@ static __constant__ double c_f64_exp10[19] = {1.0,  10.0, 100.0, 1e3,  1e4,  1e5
 constexpr double kEncUpper = 9223372036854774784.0;  // constants.hpp:18
 constexpr double kEncLower = -9223372036854774784.0;
 constexpr double kMagic = 6755399441055744.0;         // 0x0018000000000000
+// RD_SIZE_THRESHOLD_LIMIT (constants.hpp): 48 bits per value over the 32
+// samples; a best estimate at or above it sends the data to ALP-RD
+// (encoder.hpp:208-211)
+constexpr int kRDLimitBits = 48 * 32;
 
 __device__ __forceinline__ int64_t cvtt_s64(double x) {
   if (!(x >= -9223372036854775808.0 && x < 9223372036854775808.0)) return INT64_MIN;
@@ -205,7 +210,7 @@ __device__ int plain_search(const double *smp, int t, int *est_out, int *pair_ou
   }
   if (est_out) *est_out = sbest;
   if (pair_out) *pair_out = pair_class(fe, ff);
-  return sbest >= 48 * 32 ? kClassRD : pair_class(fe, ff);
+  return sbest >= kRDLimitBits ? kClassRD : pair_class(fe, ff);
 }
 
 // Labels (the plain search's class) of every vector: one warp per vector.
@@ -410,18 +415,75 @@ __device__ __forceinline__ void write_exceptions(const double *__restrict__ vec,
   }
 }
 
+// Hybrid columns: vector v as ALP-RD, with a dictionary of its own built
+// from its 32 samples (rd_encoder::init on the vector alone: the
+// first-level sample of one vector is its values at stride 32), and its
+// exceptions counted; its ALP entry is empty.
+__device__ __forceinline__ void choose_rd(const double *__restrict__ vec, const double *smp,
+                                          uint64_t *srt, size_t v, int t, EncodeSlots &sl,
+                                          RDWork &rd) {
+  rd_rank_sort<uint64_t>(reinterpret_cast<const uint64_t *>(smp), 32, srt, t);
+  const RDChoice ch = rd_find_best<uint64_t, 32>(srt, 32, t);
+  const RDLookup lk(ch);
+  const int n_exc = rd_count_exceptions<uint64_t>(reinterpret_cast<const uint64_t *>(vec), lk, t);
+  sl.exc_mask[v * 32 + t] = 0u;
+  if (t < kRDDict) rd.dicts[v * kRDDict + t] = (uint16_t)(t < ch.dsize ? ch.entry : 0u);
+  if (t == 0) {
+    sl.bw[v] = 0;
+    sl.base[v] = 0;
+    sl.fill[v] = 0;
+    sl.fac[v] = 0;
+    sl.exp[v] = 0;
+    sl.count[v] = 0;
+    rd.scheme[v] = (uint8_t)FLSGPU_SCHEME_ALP_RD;
+    rd.rbw[v] = (uint8_t)ch.rbw;
+    rd.lbw[v] = (uint8_t)ch.lbw;
+    rd.dsize[v] = (uint8_t)ch.dsize;
+    rd.dict_idx[v] = (uint32_t)v;
+    rd.count[v] = (uint16_t)n_exc;
+    rd.sizes[v] = (uint32_t)(ch.rbw * 16);
+    rd.sizes[rd.cap + v] = (uint32_t)(ch.lbw * 64);
+    rd.sizes[2 * rd.cap + v] = (uint32_t)n_exc;
+  }
+}
+
+// Hybrid columns: vector v is ALP; its ALP-RD entry is empty.
+__device__ __forceinline__ void mark_alp(size_t v, int t, RDWork &rd) {
+  if (t < kRDDict) rd.dicts[v * kRDDict + t] = 0;
+  if (t == 0) {
+    rd.scheme[v] = (uint8_t)FLSGPU_SCHEME_ALP;
+    rd.rbw[v] = 0;
+    rd.lbw[v] = 0;
+    rd.dsize[v] = 0;
+    rd.dict_idx[v] = (uint32_t)v;
+    rd.count[v] = 0;
+    rd.sizes[v] = 0;
+    rd.sizes[rd.cap + v] = 0;
+    rd.sizes[2 * rd.cap + v] = 0;
+  }
+}
+
 // Parameters of every vector, one warp per vector.  mode 0: the plain
 // search; mode 1: candidates (k per vector, network order) chosen among on
 // the samples with the reference's second-level rule (encoder.hpp:237-300),
 // and the plain search when no candidate is an ALP pair or the choice leaves
 // more than `max_exc` exceptions in the vector.  Writes the vector's
 // exponent, factor, width, base, exception count, fill integer and flags
-// (bit 0: the plain search ran as fallback; bit 1: ALP-RD territory).
+// (bit 0: the plain search ran as fallback; bit 1: ALP-RD territory, or in
+// a hybrid column: encoded as ALP-RD).
+// HYBRID: the vectors that call for ALP-RD are encoded as ALP-RD (mode 0:
+// the search's estimate reaches the ALP-RD limit, encoder.hpp:208-211;
+// mode 1: the network's top class is ALP-RD and none of its proposed ALP
+// pairs estimates below that limit on the samples).
+template <bool HYBRID>
 __global__ void __launch_bounds__(256, 4)
     k_alp_choose(const double *__restrict__ vals, size_t n_vecs, int mode,
-                 const int16_t *__restrict__ cand, int k_cand, int max_exc, EncodeSlots sl) {
+                 const int16_t *__restrict__ cand, int k_cand, int max_exc, EncodeSlots sl,
+                 RDWork rd) {
   __shared__ double s_smp[8][32];
+  __shared__ uint64_t s_srt[HYBRID ? 8 : 1][32];
   double *smp = s_smp[threadIdx.x >> 5];
+  uint64_t *srt = s_srt[HYBRID ? (threadIdx.x >> 5) : 0];
   const int t = threadIdx.x & 31;
   const size_t nw = ((size_t)gridDim.x * blockDim.x) >> 5;
   for (size_t v = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n_vecs; v += nw) {
@@ -432,8 +494,9 @@ __global__ void __launch_bounds__(256, 4)
     __syncwarp();
     int cls = -1;
     bool fallback = false, rd_net = false;
+    int best = 0;
     if (mode == 1) {
-      int best = 0, worse = 0, chosen = -1;
+      int worse = 0, chosen = -1;
       for (int c = 0; c < k_cand; ++c) {
         const int pc = cand[v * k_cand + c];
         if (pc < 0 || pc >= kClassRD) continue;
@@ -455,6 +518,15 @@ __global__ void __launch_bounds__(256, 4)
       rd_net = cand[v * k_cand] == kClassRD;
       if (cls < 0) fallback = true;
     }
+    if constexpr (HYBRID) {
+      // the network calls for ALP-RD and no proposed ALP pair gets below
+      // the limit on the samples
+      if (mode == 1 && rd_net && (cls < 0 || best >= kRDLimitBits)) {
+        choose_rd(vec, smp, srt, v, t, sl, rd);
+        if (t == 0) sl.flags[v] = 2;
+        continue;
+      }
+    }
     // A vector in ALP-RD territory is still encoded as ALP with the search's
     // best pair (most values become exceptions): the column stays an
     // ALPColumn, and the RD decision is reported through the flags.
@@ -464,7 +536,14 @@ __global__ void __launch_bounds__(256, 4)
     } else {
       pair = cls;
     }
-    const bool rd = cls == kClassRD || rd_net;
+    if constexpr (HYBRID) {
+      if (cls == kClassRD) {
+        choose_rd(vec, smp, srt, v, t, sl, rd);
+        if (t == 0) sl.flags[v] = (uint8_t)((fallback ? 1 : 0) | 2);
+        continue;
+      }
+    }
+    const bool rd_flag = HYBRID ? false : (cls == kClassRD || rd_net);
     int e = class_exp(pair), f = class_fac(pair);
     VecAnalysis a = analyze_vector(vec, e, f, t);
     // Fall back when the proposal leaves more than max_exc exceptions, ALP-RD
@@ -476,10 +555,11 @@ __global__ void __launch_bounds__(256, 4)
     if (mode == 1 && !fallback && a.n_exc > max_exc) {
       if (t == 0) {
         sl.fb_list[atomicAdd(sl.fb_count, 1u)] = (uint32_t)v;
-        sl.flags[v] = (uint8_t)(1 | (rd ? 2 : 0));
+        sl.flags[v] = (uint8_t)(1 | (rd_flag ? 2 : 0));
       }
       continue;
     }
+    if constexpr (HYBRID) mark_alp(v, t, rd);
     sl.exc_mask[v * 32 + t] = a.mask;
     if (t == 0) {
       sl.bw[v] = (uint8_t)a.bw;
@@ -488,17 +568,21 @@ __global__ void __launch_bounds__(256, 4)
       sl.fac[v] = (uint8_t)f;
       sl.exp[v] = (uint8_t)e;
       sl.count[v] = (uint16_t)a.n_exc;
-      sl.flags[v] = (uint8_t)((fallback ? 1 : 0) | (rd ? 2 : 0));
+      sl.flags[v] = (uint8_t)((fallback ? 1 : 0) | (rd_flag ? 2 : 0));
     }
   }
 }
 
 // The plain search and analysis of the vectors k_alp_choose listed (their
 // proposal left more than max_exc exceptions); one warp per listed vector.
+// HYBRID: a vector the search sends to ALP-RD is encoded as ALP-RD.
+template <bool HYBRID>
 __global__ void __launch_bounds__(256, 4)
-    k_alp_fallback(const double *__restrict__ vals, EncodeSlots sl) {
+    k_alp_fallback(const double *__restrict__ vals, EncodeSlots sl, RDWork rd) {
   __shared__ double s_smp[8][32];
+  __shared__ uint64_t s_srt[HYBRID ? 8 : 1][32];
   double *smp = s_smp[threadIdx.x >> 5];
+  uint64_t *srt = s_srt[HYBRID ? (threadIdx.x >> 5) : 0];
   const int t = threadIdx.x & 31;
   const size_t nw = ((size_t)gridDim.x * blockDim.x) >> 5;
   const size_t n = *sl.fb_count;
@@ -509,7 +593,15 @@ __global__ void __launch_bounds__(256, 4)
     smp[t] = vec[32 * t];
     __syncwarp();
     int pair;
-    plain_search(smp, t, nullptr, &pair);
+    const int cls = plain_search(smp, t, nullptr, &pair);
+    if constexpr (HYBRID) {
+      if (cls == kClassRD) {
+        choose_rd(vec, smp, srt, v, t, sl, rd);
+        if (t == 0) sl.flags[v] = 3;
+        continue;
+      }
+      mark_alp(v, t, rd);
+    }
     const int e = class_exp(pair), f = class_fac(pair);
     const VecAnalysis a = analyze_vector(vec, e, f, t);
     sl.exc_mask[v * 32 + t] = a.mask;
@@ -520,6 +612,7 @@ __global__ void __launch_bounds__(256, 4)
       sl.fac[v] = (uint8_t)f;
       sl.exp[v] = (uint8_t)e;
       sl.count[v] = (uint16_t)a.n_exc;
+      if (HYBRID) sl.flags[v] = 1;
     }
   }
 }
@@ -635,16 +728,37 @@ __global__ void __launch_bounds__(1024) k_scan_blocks(size_t nb, size_t *blk_wor
 
 // Packing at the final offsets: one warp per vector; thread t loads its 32
 // values straight from the column and writes its words of the lane stream.
+// HYBRID: ALP-RD vectors write their right parts, dictionary indices and
+// exceptions instead (rd_write_vector), and both sub-columns' offsets are
+// made final for every vector.
+template <bool HYBRID>
 __global__ void __launch_bounds__(256, 4) k_alp_pack(const double *__restrict__ vals, size_t n_vecs,
                                                   EncodeSlots sl, size_t *off_words,
                                                   size_t *off_exc, const size_t *blk_words,
                                                   const size_t *blk_exc, uint64_t *packed,
-                                                  double *exc, uint16_t *pos) {
+                                                  double *exc, uint16_t *pos, RDWork rd) {
   const int t = threadIdx.x & 31, lane = t & 15, half = t >> 4;
   const size_t nw = ((size_t)gridDim.x * blockDim.x) >> 5;
+  const size_t nb = (rd.cap + 1023) / 1024;  // stride of the ALP-RD block offsets
   for (size_t v = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n_vecs; v += nw) {
     const double *vec = vals + v * VEC;
     const size_t ow = off_words[v] + blk_words[v >> 10], oe = off_exc[v] + blk_exc[v >> 10];
+    if constexpr (HYBRID) {
+      const size_t orr = rd.offs[v] + rd.blk[v >> 10];
+      const size_t ol = rd.offs[rd.cap + v] + rd.blk[nb + (v >> 10)];
+      const size_t oer = rd.offs[2 * rd.cap + v] + rd.blk[2 * nb + (v >> 10)];
+      if (rd.scheme[v] == FLSGPU_SCHEME_ALP_RD) {
+        const RDLookup lk(rd.dicts + v * kRDDict, rd.dsize[v], rd.rbw[v]);
+        rd_write_vector<uint64_t>(reinterpret_cast<const uint64_t *>(vec), lk, rd.lbw[v], t,
+                                  rd.right + orr, rd.left + ol, rd.exc + oer, rd.pos + oer);
+      }
+      __syncwarp();
+      if (t == 0) {
+        rd.offs[v] = orr;
+        rd.offs[rd.cap + v] = ol;
+        rd.offs[2 * rd.cap + v] = oer;
+      }
+    }
     const int bw = sl.bw[v];
     const double m10e = c_f64_exp10[sl.exp[v]], mfrf = c_f64_frac[sl.fac[v]];
     const int64_t fill = sl.fill[v];
@@ -676,15 +790,25 @@ flsgpu_status run_plain_labels(const double *vals, size_t n_vecs, int16_t *label
 flsgpu_status run_alp_encode(const double *vals, size_t n_vecs, int mode, const int16_t *cand,
                              int k_cand, int max_exc, const EncodeSlots &sl, size_t *off_words,
                              size_t *off_exc, size_t *totals, uint64_t *packed, double *exc,
-                             uint16_t *pos, cudaStream_t s) {
+                             uint16_t *pos, cudaStream_t s, RDWork *rd) {
   if (!n_vecs) return FLSGPU_OK;
+  const bool hybrid = rd != nullptr;
+  const RDWork rw = hybrid ? *rd : RDWork{};
   if (mode == 1) {
     flsgpu_status st = check_cuda(cudaMemsetAsync(sl.fb_count, 0, sizeof(uint32_t), s), "memset");
     if (st) return st;
   }
-  k_alp_choose<<<warps_grid(n_vecs), 256, 0, s>>>(vals, n_vecs, mode, cand, k_cand, max_exc, sl);
+  if (hybrid)
+    k_alp_choose<true><<<warps_grid(n_vecs), 256, 0, s>>>(vals, n_vecs, mode, cand, k_cand,
+                                                          max_exc, sl, rw);
+  else
+    k_alp_choose<false><<<warps_grid(n_vecs), 256, 0, s>>>(vals, n_vecs, mode, cand, k_cand,
+                                                           max_exc, sl, rw);
   if (mode == 1) {
-    k_alp_fallback<<<warps_grid(n_vecs), 256, 0, s>>>(vals, sl);
+    if (hybrid)
+      k_alp_fallback<true><<<warps_grid(n_vecs), 256, 0, s>>>(vals, sl, rw);
+    else
+      k_alp_fallback<false><<<warps_grid(n_vecs), 256, 0, s>>>(vals, sl, rw);
     note_launch();
   }
   const size_t nb = (n_vecs + 1023) / 1024;
@@ -692,6 +816,14 @@ flsgpu_status run_alp_encode(const double *vals, size_t n_vecs, int mode, const 
                                              sl.blk_words, sl.blk_exc);
   k_scan_blocks<<<1, 1024, 0, s>>>(nb, sl.blk_words, sl.blk_exc, totals);
   note_launch();
+  if (hybrid) {
+    // the ALP-RD sub-column's right words, left words and exceptions
+    const size_t bstride = (rw.cap + 1023) / 1024;
+    k_scan_n_local<3><<<(unsigned)nb, 1024, 0, s>>>(rw.sizes, rw.cap, n_vecs, rw.offs, rw.blk,
+                                                    bstride);
+    k_scan_n_blocks<3><<<1, 1024, 0, s>>>(nb, rw.blk, bstride, rw.totals);
+    note_launch(2);
+  }
   {
     flsgpu_status st = check_cuda(cudaMemsetAsync(totals + 2, 0, 3 * sizeof(size_t), s), "memset");
     if (st) return st;
@@ -699,8 +831,12 @@ flsgpu_status run_alp_encode(const double *vals, size_t n_vecs, int mode, const 
   k_encode_stats<<<persistent_blocks(n_vecs / 32 + 1, 8, 2), 256, 0, s>>>(sl.flags, sl.bw, n_vecs,
                                                                            totals);
   note_launch();
-  k_alp_pack<<<warps_grid(n_vecs), 256, 0, s>>>(
-      vals, n_vecs, sl, off_words, off_exc, sl.blk_words, sl.blk_exc, packed, exc, pos);
+  if (hybrid)
+    k_alp_pack<true><<<warps_grid(n_vecs), 256, 0, s>>>(
+        vals, n_vecs, sl, off_words, off_exc, sl.blk_words, sl.blk_exc, packed, exc, pos, rw);
+  else
+    k_alp_pack<false><<<warps_grid(n_vecs), 256, 0, s>>>(
+        vals, n_vecs, sl, off_words, off_exc, sl.blk_words, sl.blk_exc, packed, exc, pos, rw);
   note_launch(3);
   return check_cuda(cudaGetLastError(), "alp encode");
 }

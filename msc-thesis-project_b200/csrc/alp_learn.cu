@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "alp_learn.cuh"
+#include "rd_encode.cuh"
 #include "umma.cuh"
 
 namespace flsb200 {
@@ -712,6 +713,8 @@ struct flsgpu_alp_encoder {
   double *exc = nullptr;
   uint16_t *pos = nullptr;
   size_t *exc_offs = nullptr, *vec_offs = nullptr;
+  // ALP-RD encoder workspace (its column, and the RD part of hybrid columns)
+  RDWork rd;
 };
 
 namespace {
@@ -931,6 +934,54 @@ flsgpu_status propose_layered(flsgpu_alp_encoder *e, const double *vals, size_t 
 
 }  // namespace
 
+namespace flsb200 {
+
+template <typename T>
+static flsgpu_status alprd_encode(flsgpu_alp_encoder *e, const T *d_values, size_t n_values,
+                                  uint32_t rowgroup_vecs, flsgpu_alprd_encode_result *out,
+                                  flsgpu_stream stream) {
+  if (!e || !d_values || !out || (n_values % VEC) || rowgroup_vecs < 1 || rowgroup_vecs > 100)
+    return set_error(FLSGPU_ERR_INVALID_ARGUMENT,
+                     "ALP-RD encode: null argument, n_values not a multiple of 1024, or "
+                     "rowgroup_vecs outside 1..100");
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t n_vecs = n_values / VEC;
+  flsgpu_status st = rd_work_reserve(e->rd, n_vecs);
+  if (st) return st;
+  if ((st = run_rd_encode<T>(d_values, n_vecs, (int)rowgroup_vecs, e->rd, s))) return st;
+  size_t tot[3] = {0, 0, 0};
+  if (n_vecs &&
+      ((st = check_cuda(cudaMemcpyAsync(tot, e->rd.totals, sizeof(tot), cudaMemcpyDeviceToHost, s),
+                        "copy")) ||
+       (st = check_cuda(cudaStreamSynchronize(s), "sync"))))
+    return st;
+  std::memset(out, 0, sizeof(*out));
+  flsgpu_alprd_column &c = out->column;
+  RDWork &w = e->rd;
+  c.n_values = n_values;
+  c.right = flsgpu_bp_column{n_values, n_vecs, w.right, w.rbw, w.offs};
+  c.left = flsgpu_bp_column{n_values, n_vecs, w.left, w.lbw, w.offs + w.cap};
+  c.dictionaries = w.dicts;
+  c.dictionary_indices = w.dict_idx;
+  c.n_exceptions = tot[2];
+  c.exceptions_offsets = w.offs + 2 * w.cap;
+  c.exceptions = w.exc;
+  c.positions = w.pos;
+  c.counts = w.count;
+  const size_t n_dict = (n_vecs + rowgroup_vecs - 1) / rowgroup_vecs;
+  out->n_right_words = tot[0];
+  out->n_left_words = tot[1];
+  out->n_exceptions = tot[2];
+  out->n_dictionaries = n_dict;
+  // packed words, 4 B per exception (left part + position), 16 B per
+  // dictionary, and per vector the two widths, three offsets, the
+  // dictionary index and the exception count (32 B)
+  out->compressed_bytes = tot[0] * sizeof(T) + tot[1] * 2 + tot[2] * 4 + n_dict * 16 + n_vecs * 32;
+  return FLSGPU_OK;
+}
+
+}  // namespace flsb200
+
 extern "C" {
 
 flsgpu_status flsgpu_alp_encoder_create(uint32_t seed, flsgpu_alp_encoder **out) {
@@ -980,6 +1031,7 @@ void flsgpu_alp_encoder_destroy(flsgpu_alp_encoder *e) {
   if (!e) return;
   free_acts(e);
   free_enc(e);
+  rd_work_free(e->rd);
   for (void *p : {(void *)e->w, (void *)e->m, (void *)e->v, (void *)e->g, (void *)e->w1b,
                   (void *)e->w2b, (void *)e->w3b, (void *)e->w2t, (void *)e->w3t, (void *)e->status})
     if (p) cudaFree(p);
@@ -1217,6 +1269,90 @@ flsgpu_status flsgpu_alp_encode_f64(flsgpu_alp_encoder *e, const double *d_value
   out->n_fallback = fb;
   out->n_rd = rd;
   out->mean_bit_width = n_vecs ? (double)bwsum / (double)n_vecs : 0.0;
+  return FLSGPU_OK;
+}
+
+flsgpu_status flsgpu_alprd_encode_f64(flsgpu_alp_encoder *e, const double *d_values,
+                                      size_t n_values, uint32_t rowgroup_vecs,
+                                      flsgpu_alprd_encode_result *out, flsgpu_stream stream) {
+  return alprd_encode<double>(e, d_values, n_values, rowgroup_vecs, out, stream);
+}
+
+flsgpu_status flsgpu_alprd_encode_f32(flsgpu_alp_encoder *e, const float *d_values,
+                                      size_t n_values, uint32_t rowgroup_vecs,
+                                      flsgpu_alprd_encode_result *out, flsgpu_stream stream) {
+  return alprd_encode<float>(e, d_values, n_values, rowgroup_vecs, out, stream);
+}
+
+flsgpu_status flsgpu_alp_encode_hybrid_f64(flsgpu_alp_encoder *e, const double *d_values,
+                                           size_t n_values, uint32_t mode,
+                                           flsgpu_alp_hybrid_encode_result *out,
+                                           flsgpu_stream stream) {
+  if (!e || !d_values || !out || (n_values % VEC) || mode > 1)
+    return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "hybrid encode: bad arguments");
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t n_vecs = n_values / VEC;
+  flsgpu_status st = ensure_vecs(e, n_vecs);
+  if (st || (st = rd_work_reserve(e->rd, n_vecs))) return st;
+  if (mode == 1 && (st = propose(e, d_values, n_vecs, 3, s))) return st;
+  if ((st = run_alp_encode(d_values, n_vecs, (int)mode, e->cand, 3, 30, e->sl, e->off_words,
+                           e->off_exc, e->totals, e->packed, e->exc, e->pos, s, &e->rd)))
+    return st;
+  size_t tot[5] = {0, 0, 0, 0, 0}, rtot[3] = {0, 0, 0};
+  if ((st = check_cuda(cudaMemcpyAsync(tot, e->totals, sizeof(tot), cudaMemcpyDeviceToHost, s), "copy")) ||
+      (st = check_cuda(cudaMemcpyAsync(rtot, e->rd.totals, sizeof(rtot), cudaMemcpyDeviceToHost, s),
+                       "copy")) ||
+      (st = check_cuda(cudaStreamSynchronize(s), "sync")))
+    return st;
+  std::memset(out, 0, sizeof(*out));
+  flsgpu_alphybrid_column &h = out->column;
+  h.n_values = n_values;
+  flsgpu_alp_column &c = h.alp;
+  c.n_values = n_values;
+  c.ffor.n_values = n_values;
+  c.ffor.bp.n_values = n_values;
+  c.ffor.bp.n_vecs = n_vecs;
+  c.ffor.bp.packed_array = e->packed;
+  c.ffor.bp.bit_widths = e->sl.bw;
+  c.ffor.bp.vector_offsets = e->off_words;
+  c.ffor.bases = e->sl.base;
+  c.factor_indices = e->sl.fac;
+  c.fraction_indices = e->sl.exp;
+  c.n_exceptions = tot[1];
+  c.exceptions_offsets = e->off_exc;
+  c.exceptions = e->exc;
+  c.positions = e->pos;
+  c.counts = e->sl.count;
+  RDWork &w = e->rd;
+  flsgpu_alprd_column &r = h.rd;
+  r.n_values = n_values;
+  r.right = flsgpu_bp_column{n_values, n_vecs, w.right, w.rbw, w.offs};
+  r.left = flsgpu_bp_column{n_values, n_vecs, w.left, w.lbw, w.offs + w.cap};
+  r.dictionaries = w.dicts;
+  r.dictionary_indices = w.dict_idx;
+  r.n_exceptions = rtot[2];
+  r.exceptions_offsets = w.offs + 2 * w.cap;
+  r.exceptions = w.exc;
+  r.positions = w.pos;
+  r.counts = w.count;
+  h.schemes = w.scheme;
+  const size_t n_rd = tot[3], n_alp = n_vecs - n_rd;
+  out->n_alp_vectors = n_alp;
+  out->n_rd_vectors = n_rd;
+  out->n_packed_words = tot[0];
+  out->n_exceptions = tot[1];
+  out->n_right_words = rtot[0];
+  out->n_left_words = rtot[1];
+  out->n_rd_exceptions = rtot[2];
+  out->n_fallback = tot[2];
+  out->mean_bit_width = n_alp ? (double)tot[4] / (double)n_alp : 0.0;
+  out->d_flags = e->sl.flags;
+  // ALP vectors as alp::encode accounts them (alp-bindings.cu:19-43: packed
+  // bytes, 10 B per exception, 11 B per vector); ALP-RD vectors: packed
+  // words, 4 B per exception, a 16 B dictionary and 32 B of metadata; one
+  // scheme byte per vector
+  out->compressed_bytes = tot[0] * 8 + tot[1] * 10 + n_alp * 11 + rtot[0] * 8 + rtot[1] * 2 +
+                          rtot[2] * 4 + n_rd * 48 + n_vecs;
   return FLSGPU_OK;
 }
 

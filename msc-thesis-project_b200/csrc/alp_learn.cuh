@@ -51,11 +51,15 @@ flsgpu_status run_plain_labels(const double *vals, size_t n_vecs, int16_t *label
                                cudaStream_t s);
 // parameter choice (mode 0: plain search; 1: verified proposals with
 // fallback) and analysis, scan of the per-vector sizes (totals[0] = packed
-// words, totals[1] = exceptions), then packing into packed / exc / pos
+// words, totals[1] = exceptions), then packing into packed / exc / pos.
+// With `rd` (hybrid columns) the vectors that call for ALP-RD are encoded
+// into the ALP-RD workspace instead (rd->totals: right words, left words,
+// exceptions; rd->scheme per vector).
+struct RDWork;
 flsgpu_status run_alp_encode(const double *vals, size_t n_vecs, int mode, const int16_t *cand,
                              int k_cand, int max_exc, const EncodeSlots &sl, size_t *off_words,
                              size_t *off_exc, size_t *totals, uint64_t *packed, double *exc,
-                             uint16_t *pos, cudaStream_t s);
+                             uint16_t *pos, cudaStream_t s, RDWork *rd = nullptr);
 
 struct GemmArgs {
   const __nv_bfloat16 *A;

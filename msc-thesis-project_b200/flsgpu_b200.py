@@ -704,6 +704,22 @@ class EncodeResultC(C.Structure):
                 ("mean_bit_width", C.c_double)]
 
 
+class HybridColumnC(C.Structure):
+    _fields_ = [("n_values", SZ), ("alp", ALPColumnC), ("rd", ALPRDColumnC), ("schemes", P)]
+
+
+class HybridEncodeResultC(C.Structure):
+    _fields_ = [("column", HybridColumnC), ("n_alp_vectors", SZ), ("n_rd_vectors", SZ),
+                ("n_packed_words", SZ), ("n_exceptions", SZ), ("n_right_words", SZ),
+                ("n_left_words", SZ), ("n_rd_exceptions", SZ), ("compressed_bytes", SZ),
+                ("n_fallback", SZ), ("mean_bit_width", C.c_double), ("d_flags", P)]
+
+
+class RDEncodeResultC(C.Structure):
+    _fields_ = [("column", ALPRDColumnC), ("n_right_words", SZ), ("n_left_words", SZ),
+                ("n_exceptions", SZ), ("n_dictionaries", SZ), ("compressed_bytes", SZ)]
+
+
 class AlpEncoder:
     """GPU ALP encoder for f64 columns; mode 0 = plain per-vector search,
     mode 1 = learned proposal verified on samples, with fallback."""
@@ -726,6 +742,25 @@ class AlpEncoder:
         _check(_fn("flsgpu_alp_encode_f64")(self.h, P(_ptr(values)), SZ(values.numel()),
                                            C.c_uint32(mode), C.byref(r),
                                            P(_stream_handle(stream))))
+        return r
+
+    def encode_hybrid(self, values, mode: int, stream=None) -> HybridEncodeResultC:
+        """Hybrid ALP / ALP-RD encode of an f64 column (mode 0 plain search,
+        1 learned proposal); ALP-RD vectors get a dictionary of their own."""
+        r = HybridEncodeResultC()
+        _check(_fn("flsgpu_alp_encode_hybrid_f64")(self.h, P(_ptr(values)), SZ(values.numel()),
+                                                  C.c_uint32(mode), C.byref(r),
+                                                  P(_stream_handle(stream))))
+        return r
+
+    def encode_rd(self, values, rowgroup_vecs: int = 100, stream=None) -> RDEncodeResultC:
+        """ALP-RD encode of an f64 (float64 tensor) or f32 (float32 tensor)
+        column, one dictionary per rowgroup of rowgroup_vecs vectors."""
+        r = RDEncodeResultC()
+        suf = "f64" if values.element_size() == 8 else "f32"
+        _check(_fn(f"flsgpu_alprd_encode_{suf}")(self.h, P(_ptr(values)), SZ(values.numel()),
+                                                C.c_uint32(rowgroup_vecs), C.byref(r),
+                                                P(_stream_handle(stream))))
         return r
 
     def propose(self, values, k=3, stream=None, layered=False):
@@ -779,6 +814,20 @@ def encoded_column(res: EncodeResultC, n_values: int, keep=None) -> DeviceColumn
     """The encoder's output as a decodable DeviceColumn (device arrays owned
     by the encoder; valid until its next encode)."""
     return DeviceColumn("alp", "f64", n_values, res.column, {"_owner": keep} if keep else {},
+                        int(res.n_packed_words))
+
+
+def rd_encoded_column(res: RDEncodeResultC, n_values: int, dtype: str = "f64",
+                      keep=None) -> DeviceColumn:
+    """The ALP-RD encoder's output as a decodable DeviceColumn (arrays owned
+    by the encoder; valid until its next encode)."""
+    return DeviceColumn("alprd", dtype, n_values, res.column, {"_owner": keep} if keep else {},
+                        int(res.n_right_words))
+
+
+def hybrid_column(res: HybridEncodeResultC, n_values: int, keep=None) -> DeviceColumn:
+    """The hybrid encoder's output as a decodable DeviceColumn."""
+    return DeviceColumn("alphybrid", "f64", n_values, res.column, {"_owner": keep} if keep else {},
                         int(res.n_packed_words))
 
 
