@@ -56,6 +56,7 @@ typedef struct CUstream_st *flsgpu_stream;
 #define FLSGPU_BAD_OFFSET 0x2u         /* packed offset + size beyond bound */
 #define FLSGPU_BAD_PARAMETER_INDEX 0x4u /* ALP factor / exponent index */
 #define FLSGPU_BAD_EXCEPTION 0x8u      /* exception count / position range */
+#define FLSGPU_WAIT_TIMEOUT 0x10u      /* a bounded device wait (staged copy) gave up */
 
 /* reference enums::Unpacker (src/engine/enums.cuh:21-41), same order */
 typedef enum flsgpu_unpacker {
@@ -92,6 +93,11 @@ typedef enum flsgpu_variant {
                                     for 32-bit lanes, 1 for 64-bit lanes */
   FLSGPU_VARIANT_OCCUPANCY = 2,  /* register-capped for twice the resident
                                     blocks (more loads in flight) */
+  FLSGPU_VARIANT_STAGED = 3,     /* 64-bit lanes: each vector's packed words
+                                    (width <= 32) copied into a per-warp
+                                    shared-memory slot by a bulk copy one
+                                    vector ahead, unpacked from there; other
+                                    widths and 32-bit lanes as REGS */
   FLSGPU_VARIANT_COUNT
 } flsgpu_variant;
 

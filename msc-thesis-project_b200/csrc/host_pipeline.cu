@@ -134,6 +134,25 @@ static flsgpu_status stage_alp(flsgpu_host_pipeline *p, int sl, const flsgpu_alp
   return FLSGPU_OK;
 }
 
+// A staged chunk is decoded through the library's own C entry points (the
+// kernels are compiled once, in their translation units).
+static flsgpu_status decode_chunk(const flsgpu_ffor_column *c, uint32_t *o,
+                                  const flsgpu_decode_opts *op, flsgpu_stream s) {
+  return flsgpu_decompress_ffor_u32(c, o, op, s);
+}
+static flsgpu_status decode_chunk(const flsgpu_ffor_column *c, uint64_t *o,
+                                  const flsgpu_decode_opts *op, flsgpu_stream s) {
+  return flsgpu_decompress_ffor_u64(c, o, op, s);
+}
+static flsgpu_status decode_chunk(const flsgpu_alp_column *c, float *o,
+                                  const flsgpu_decode_opts *op, flsgpu_stream s) {
+  return flsgpu_decompress_alp_f32(c, o, op, s);
+}
+static flsgpu_status decode_chunk(const flsgpu_alp_column *c, double *o,
+                                  const flsgpu_decode_opts *op, flsgpu_stream s) {
+  return flsgpu_decompress_alp_f64(c, o, op, s);
+}
+
 // The chunk loop: stage (stream in), decode (stream comp), copy out
 // (stream out); slot reuse waits on the decode (inputs) and the copy out
 // (output) of the chunk two before.
@@ -187,7 +206,7 @@ static flsgpu_status host_ffor(flsgpu_host_pipeline *p, const flsgpu_ffor_column
         dc.n_values = n;
         dc.bp.n_values = n;
         dc.bp.n_vecs = (n + 1023) / 1024;
-        return decompress<T, K_FFOR>(&dc, d_out, o, (flsgpu_stream)p->comp);
+        return decode_chunk(&dc, d_out, o, (flsgpu_stream)p->comp);
       });
 }
 
@@ -224,7 +243,7 @@ static flsgpu_status host_alp(flsgpu_host_pipeline *p, const flsgpu_alp_column *
         dc.ffor.n_values = n;
         dc.ffor.bp.n_values = n;
         dc.ffor.bp.n_vecs = (n + 1023) / 1024;
-        return decompress<T, K_ALP>(&dc, d_out, o, (flsgpu_stream)p->comp);
+        return decode_chunk(&dc, d_out, o, (flsgpu_stream)p->comp);
       });
 }
 

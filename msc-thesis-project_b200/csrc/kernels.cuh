@@ -664,6 +664,9 @@ template <typename T> constexpr int type_code() {
        : std::is_same<T, float>::value ? 2 : 3;
 }
 
+// The staged decode of 64-bit lanes (staged.cuh).
+template <typename T, int KIND> flsgpu_status launch_staged(const KernelParams &p, cudaStream_t s);
+
 template <typename T, int KIND, int SINK> struct Launch {
   static constexpr bool STAGE = (KIND == K_ALP || KIND == K_ALPX) && SINK != S_STORE;
   static size_t smem() { return STAGE ? (size_t)8 * VEC * sizeof(T) : 0; }
@@ -699,6 +702,9 @@ template <typename T, int KIND, int SINK> struct Launch {
     if constexpr (SINK == S_STORE) {
       if (variant == FLSGPU_VARIANT_AUTO) variant = (uint32_t)tuned_variant(type_code<T>(), KIND);
       if (variant == FLSGPU_VARIANT_OCCUPANCY) return launch<VAR_OCC>(p, s);
+      if constexpr (sizeof(T) == 8) {
+        if (variant == FLSGPU_VARIANT_STAGED) return launch_staged<T, KIND>(p, s);
+      }
     }
     return launch<0>(p, s);
   }
@@ -996,3 +1002,5 @@ static flsgpu_status compute(const Col *col, uint32_t n_rep, uint8_t *d_out,
 }
 
 }  // namespace flsb200
+
+#include "staged.cuh"

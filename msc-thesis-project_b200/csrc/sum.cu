@@ -3,6 +3,15 @@
 
 #include "kernels.cuh"
 
+namespace flsb200 {
+// The f64 ALP decode-and-sum, shared with the allocation-free entry point
+// (sum_noalloc.cu), which passes its static scratch as the partials.
+flsgpu_status sum_alp_f64_impl(const flsgpu_alp_column *c, double *d_sum, double *d_partials,
+                               const flsgpu_decode_opts *op, flsgpu_stream s) {
+  return sum_f64<K_ALP>(c, d_sum, d_partials, op, s);
+}
+}  // namespace flsb200
+
 using namespace flsb200;
 
 extern "C" {
@@ -19,7 +28,7 @@ flsgpu_status flsgpu_sum_ffor_u64(const flsgpu_ffor_column *c, uint64_t *d_sum,
 
 flsgpu_status flsgpu_sum_alp_f64(const flsgpu_alp_column *c, double *d_sum, double *d_partials,
                                  const flsgpu_decode_opts *op, flsgpu_stream s) {
-  return sum_f64<K_ALP>(c, d_sum, d_partials, op, s);
+  return sum_alp_f64_impl(c, d_sum, d_partials, op, s);
 }
 
 flsgpu_status flsgpu_sum_alpx_f64(const flsgpu_alpx_column *c, double *d_sum, double *d_partials,

@@ -40,6 +40,10 @@ constexpr size_t kNoAllocScratch = kNoAllocMaxVectors + (kNoAllocMaxVectors + 20
 
 static __device__ __align__(256) double g_noalloc_partials[kNoAllocScratch];
 
+// the decode-and-sum itself (sum.cu)
+flsgpu_status sum_alp_f64_impl(const flsgpu_alp_column *c, double *d_sum, double *d_partials,
+                               const flsgpu_decode_opts *op, flsgpu_stream s);
+
 // In host code g_noalloc_partials names a host-side stand-in, not device
 // memory: its device address is looked up with the device current, and
 // cached per device together with the id of the context it was taken in.
@@ -117,7 +121,7 @@ flsgpu_status flsgpu_sum_alp_f64_noalloc(const flsgpu_alp_column *c, double *d_s
   double *scratch = nullptr;
   flsgpu_status st = noalloc_scratch(&scratch);
   if (st) return st;
-  return sum_f64<K_ALP>(c, d_sum, scratch, op, s);
+  return sum_alp_f64_impl(c, d_sum, scratch, op, s);
 }
 
 }  // extern "C"

@@ -41,7 +41,7 @@ UNPACKERS = ["Dummy", "OldFls", "SwitchCase", "Stateless", "StatelessBranchless"
              "StatefulBranchless"]
 PATCHERS = ["None", "Dummy", "Stateless", "Stateful", "Naive", "NaiveBranchless",
             "PrefetchPosition", "PrefetchAll", "PrefetchAllBranchless"]
-VARIANT_AUTO, VARIANT_REGS, VARIANT_OCCUPANCY = 0, 1, 2
+VARIANT_AUTO, VARIANT_REGS, VARIANT_OCCUPANCY, VARIANT_STAGED = 0, 1, 2, 3
 
 
 class FlsgpuError(RuntimeError):
@@ -535,8 +535,9 @@ def autotune(values_32: int = 2 ** 26, values_64: int = 2 ** 25, reps: int = 5, 
 
     report = {"ffor": {}, "alp": {}}
     table = {"variant": {}, "prefetch": {}}
-    variants = (VARIANT_REGS, VARIANT_OCCUPANCY)
     for bits, n in ((32, values_32), (64, values_64)):
+        # the staged decode exists for 64-bit lanes only
+        variants = (VARIANT_REGS, VARIANT_OCCUPANCY) + ((VARIANT_STAGED,) if bits == 64 else ())
         n -= n % 1024
         out = torch.empty(n, dtype=torch.int32 if bits == 32 else torch.int64, device=dev)
         per = {v: {} for v in variants}
@@ -565,6 +566,7 @@ def autotune(values_32: int = 2 ** 26, values_64: int = 2 ** 25, reps: int = 5, 
         del out
     for bits, n in ((32, values_32), (64, values_64)):
         n -= n % 1024
+        variants = (VARIANT_REGS, VARIANT_OCCUPANCY) + ((VARIANT_STAGED,) if bits == 64 else ())
         widths = alp_widths or ((8, 12, 16, 20, 24, 28) if bits == 32 else (8, 16, 20, 24, 32, 40, 48))
         out = torch.empty(n, dtype=torch.float32 if bits == 32 else torch.float64, device=dev)
         tot = {v: 0.0 for v in variants}

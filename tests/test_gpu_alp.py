@@ -35,7 +35,7 @@ def _check(cuda, col, n_vecs, f64, extended=False, patcher=7, variant=F.VARIANT_
 
 @pytest.mark.parametrize("f64", [True, False])
 @pytest.mark.parametrize("extended", [False, True])
-@pytest.mark.parametrize("variant", [F.VARIANT_REGS, F.VARIANT_OCCUPANCY])
+@pytest.mark.parametrize("variant", [F.VARIANT_REGS, F.VARIANT_OCCUPANCY, F.VARIANT_STAGED])
 def test_alp_widths_and_exception_counts(cuda, f64, extended, variant):
     bits = 64 if f64 else 32
     for ec in [0, 1, 5, 10, 33, 70]:

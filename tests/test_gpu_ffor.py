@@ -43,7 +43,8 @@ def test_bp_every_width(cuda, bits):
 
 
 @pytest.mark.parametrize("bits", [32, 64])
-@pytest.mark.parametrize("variant", [F.VARIANT_AUTO, F.VARIANT_REGS, F.VARIANT_OCCUPANCY])
+@pytest.mark.parametrize("variant", [F.VARIANT_AUTO, F.VARIANT_REGS, F.VARIANT_OCCUPANCY,
+                                     F.VARIANT_STAGED])
 def test_ffor_mixed_widths(cuda, bits, variant):
     ut = np.uint64 if bits == 64 else np.uint32
     c = colgen.random_ffor(7 + bits, 3000, bits, range(bits + 1))
@@ -150,3 +151,37 @@ def test_corrupt_metadata_is_flagged_not_faulted(cuda, bits):
     status.zero_()
     F.decompress(_col(c, cuda), o=F.opts(d_status=status, n_packed_values=c["packed"].size - 1))
     assert int(status.item()) & F.BAD_OFFSET
+
+
+@pytest.mark.parametrize("bp", [False, True])
+def test_staged_decode_every_width_and_unaligned_vectors(cuda, bp):
+    """The staged u64 decode (packed words brought into shared memory by bulk
+    copies): every width 0..64, ragged tails, and a column whose vectors'
+    packed words are not 16-byte aligned (odd word offsets), which take the
+    register-held path."""
+    import torch
+    for w in range(65):
+        c = colgen.random_ffor(700 + w, 7, 64, [w], n_values=7 * 1024 - 5)
+        got = _host(F.decompress(_col(c, cuda, bp), o=F.opts(variant=F.VARIANT_STAGED)), np.uint64)
+        want = (B.decode_bp(c["packed"], c["bit_widths"], c["vector_offsets"], 64) if bp else
+                B.decode_ffor(c["packed"], c["bit_widths"], c["vector_offsets"], c["bases"], 64))
+        assert np.array_equal(got, want[:c["n_values"]]), w
+    # odd word offsets: one spare word before every vector's packed words
+    c = colgen.random_ffor(31, 40, 64, range(65))
+    n_vecs = 40
+    offs = c["vector_offsets"].astype(np.int64) + np.arange(1, n_vecs + 1)
+    packed = np.zeros(int(c["packed"].size) + n_vecs + 1, np.uint64)
+    for v in range(n_vecs):
+        n = int(c["bit_widths"][v]) * 16
+        o0 = int(c["vector_offsets"][v])
+        packed[offs[v]:offs[v] + n] = c["packed"][o0:o0 + n]
+    d = F.make_ffor_column(packed, c["bit_widths"], offs.astype(np.uint64),
+                           None if bp else c["bases"], c["n_values"], cuda)
+    got = _host(F.decompress(d, o=F.opts(variant=F.VARIANT_STAGED)), np.uint64)
+    want = (B.decode_bp(c["packed"], c["bit_widths"], c["vector_offsets"], 64) if bp else
+            B.decode_ffor(c["packed"], c["bit_widths"], c["vector_offsets"], c["bases"], 64))
+    assert np.array_equal(got, want)
+    # a status word stays clear (no wait gave up)
+    status = torch.zeros(1, dtype=torch.int32, device=cuda)
+    F.decompress(d, o=F.opts(variant=F.VARIANT_STAGED, d_status=status))
+    assert int(status.item()) == 0

@@ -18,7 +18,8 @@ def test_autotune_small_sizes_installs_a_complete_table(cuda):
         t = r["table"]
         for tn, kn in (("u32", "ffor"), ("u32", "bp"), ("u64", "ffor"), ("u64", "bp"),
                        ("f32", "alp"), ("f32", "alpx"), ("f64", "alp"), ("f64", "alpx")):
-            assert t["variant"][(tn, kn)] in (F.VARIANT_REGS, F.VARIANT_OCCUPANCY)
+            assert t["variant"][(tn, kn)] in (F.VARIANT_REGS, F.VARIANT_OCCUPANCY,
+                                              F.VARIANT_STAGED)
         assert set(t["prefetch"]) == {32, 64}
         assert len(r["report"]["ffor"]["u32"]["gbs"][str(F.VARIANT_REGS)]) == 33
         assert len(r["report"]["ffor"]["u64"]["gbs"][str(F.VARIANT_OCCUPANCY)]) == 65
