@@ -231,6 +231,24 @@ flsgpu_status flsgpu_decompress_alphybrid_f64(const flsgpu_alphybrid_column *col
                                               double *d_out, const flsgpu_decode_opts *opts,
                                               flsgpu_stream stream);
 
+/* ---- lane-divided exception layout on the GPU
+ *      (host::ALPColumn::create_extended_column and
+ *      convert_exceptions_to_lane_divided_format, src/flsgpu/structs.cuh:
+ *      231-308, which the reference runs on the host).  Writes the
+ *      exceptions of `src` regrouped by FastLanes lane (order kept within a
+ *      lane) to d_exceptions / d_positions (src->n_exceptions elements each)
+ *      and per vector and lane (count << 10) | offset to d_offsets_counts
+ *      (n_vecs * 32 (f32) or * 16 (f64) elements; 16 bits, so a 64-bit lane
+ *      with 64 exceptions wraps as in the reference), and fills *dst: the
+ *      extended column sharing src's packed words, metadata and exception
+ *      offsets.  Enqueued on `stream`. ------------------------------------ */
+flsgpu_status flsgpu_alp_to_extended_f32(const flsgpu_alp_column *src, float *d_exceptions,
+                                         uint16_t *d_positions, uint16_t *d_offsets_counts,
+                                         flsgpu_alpx_column *dst, flsgpu_stream stream);
+flsgpu_status flsgpu_alp_to_extended_f64(const flsgpu_alp_column *src, double *d_exceptions,
+                                         uint16_t *d_positions, uint16_t *d_offsets_counts,
+                                         flsgpu_alpx_column *dst, flsgpu_stream stream);
+
 /* ---- FastLanes packing, the encoder side (fls::ffor src/fls/ffor.cpp:
  *      29861, fls::pack src/fls/pack.cpp:29731, base / width rule of
  *      analyze_ffor src/alp/encoder.hpp:104-115; the reference packs on the

@@ -22,8 +22,11 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
+#include <random>
 #include <stdexcept>
 #include <string>
 #include <type_traits>
@@ -180,8 +183,15 @@ template <typename T, bool EXTENDED> struct ALPColumnBase {
   size_t get_n_values() const { return ffor.bp.n_values; }
   size_t get_n_vecs() const { return ffor.bp.get_n_vecs(); }
 };
+template <typename T> struct ALPExtendedColumn;
 template <typename T> struct ALPColumn : ALPColumnBase<T, false> {
   using DeviceColumnT = device::ALPColumn<T>;
+  // create_extended_column (structs.cuh:231-308): the same column with its
+  // exceptions regrouped by lane, converted on the GPU
+  // (flsgpu_alp_to_extended_*).  The result shares ffor and the per-vector
+  // metadata with this column; its exceptions, positions and
+  // offsets_counts are new malloc'ed host arrays (release with free()).
+  ALPExtendedColumn<T> create_extended_column() const;
   device::ALPColumn<T> copy_to_device() const {
     const size_t nv = this->get_n_vecs();
     return device::ALPColumn<T>{this->get_n_values(), this->ffor.copy_to_device(), nullptr,
@@ -207,6 +217,53 @@ template <typename T> struct ALPExtendedColumn : ALPColumnBase<T, true> {
         detail::to_device(this->counts_or_offsets_counts, nv * nl)};
   }
 };
+
+template <typename T> ALPExtendedColumn<T> ALPColumn<T>::create_extended_column() const {
+  const size_t nv = this->get_n_vecs();
+  const size_t nl = 1024 / (8 * sizeof(T));
+  const size_t ne = this->n_exceptions;
+  // the conversion reads only the exception arrays, counts and offsets
+  flsgpu_alp_column d{};
+  d.n_values = this->get_n_values();
+  d.n_exceptions = ne;
+  d.exceptions_offsets = detail::to_device(this->exceptions_offsets, nv);
+  d.exceptions = detail::to_device(this->exceptions, ne);
+  d.positions = detail::to_device(this->positions, ne);
+  d.counts = detail::to_device(this->counts_or_offsets_counts, nv);
+  T *d_exc = nullptr;
+  uint16_t *d_pos = nullptr, *d_oc = nullptr;
+  detail::cuda_check(cudaMalloc(reinterpret_cast<void **>(&d_exc), (ne ? ne : 1) * sizeof(T)), "cudaMalloc");
+  detail::cuda_check(cudaMalloc(reinterpret_cast<void **>(&d_pos), (ne ? ne : 1) * 2), "cudaMalloc");
+  detail::cuda_check(cudaMalloc(reinterpret_cast<void **>(&d_oc), (nv ? nv * nl : 1) * 2), "cudaMalloc");
+  flsgpu_alpx_column x{};
+  flsgpu_status st;
+  if constexpr (sizeof(T) == 8)
+    st = flsgpu_alp_to_extended_f64(&d, d_exc, d_pos, d_oc, &x, nullptr);
+  else
+    st = flsgpu_alp_to_extended_f32(&d, d_exc, d_pos, d_oc, &x, nullptr);
+  ALPExtendedColumn<T> out{};
+  out.ffor = this->ffor;
+  out.factor_indices = this->factor_indices;
+  out.fraction_indices = this->fraction_indices;
+  out.n_exceptions = ne;
+  out.exceptions_offsets = this->exceptions_offsets;
+  out.exceptions = static_cast<T *>(malloc(sizeof(T) * (ne ? ne : 1)));
+  out.positions = static_cast<uint16_t *>(malloc(2 * (ne ? ne : 1)));
+  out.counts_or_offsets_counts = static_cast<uint16_t *>(malloc(2 * (nv ? nv * nl : 1)));
+  cudaError_t e = st == FLSGPU_OK ? cudaDeviceSynchronize() : cudaSuccess;
+  if (st == FLSGPU_OK && e == cudaSuccess) {
+    if (ne) e = cudaMemcpy(out.exceptions, d_exc, sizeof(T) * ne, cudaMemcpyDeviceToHost);
+    if (ne && e == cudaSuccess) e = cudaMemcpy(out.positions, d_pos, 2 * ne, cudaMemcpyDeviceToHost);
+    if (nv && e == cudaSuccess)
+      e = cudaMemcpy(out.counts_or_offsets_counts, d_oc, 2 * nv * nl, cudaMemcpyDeviceToHost);
+  }
+  for (void *p : {(void *)d.exceptions_offsets, (void *)d.exceptions, (void *)d.positions,
+                  (void *)d.counts, (void *)d_exc, (void *)d_pos, (void *)d_oc})
+    cudaFree(p);
+  detail::check(st);
+  detail::cuda_check(e, "create_extended_column");
+  return out;
+}
 
 // host::free_column(device::...) (structs.cuh:367-400)
 template <typename T> void free_column(device::BPColumn<T> c) {
@@ -294,6 +351,75 @@ bool query_column(const ColumnT column, const unsigned unpack_n_vectors,
     flsgpu::detail::check(detail::qry(column, magic_value, d.p, &o));
     flsgpu::detail::cuda_check(cudaDeviceSynchronize(), "query_column");
   }
+  uint8_t h = 0;
+  flsgpu::detail::cuda_check(cudaMemcpy(&h, d.p, 1, cudaMemcpyDeviceToHost), "copy");
+  return h != 0;
+}
+
+namespace detail {
+inline flsgpu_status qmc(const flsgpu::device::FFORColumn<uint32_t> *c, uint32_t n, uint32_t v, uint8_t *o, const flsgpu_decode_opts *op) { return flsgpu_query_multi_column_ffor_u32(reinterpret_cast<const flsgpu_ffor_column *>(c), n, v, o, op, nullptr); }
+inline flsgpu_status qmc(const flsgpu::device::FFORColumn<uint64_t> *c, uint32_t n, uint64_t v, uint8_t *o, const flsgpu_decode_opts *op) { return flsgpu_query_multi_column_ffor_u64(reinterpret_cast<const flsgpu_ffor_column *>(c), n, v, o, op, nullptr); }
+inline flsgpu_status qmc(const flsgpu::device::ALPColumn<float> *c, uint32_t n, float v, uint8_t *o, const flsgpu_decode_opts *op) { return flsgpu_query_multi_column_alp_f32(reinterpret_cast<const flsgpu_alp_column *>(c), n, v, o, op, nullptr); }
+inline flsgpu_status qmc(const flsgpu::device::ALPColumn<double> *c, uint32_t n, double v, uint8_t *o, const flsgpu_decode_opts *op) { return flsgpu_query_multi_column_alp_f64(reinterpret_cast<const flsgpu_alp_column *>(c), n, v, o, op, nullptr); }
+template <typename C> auto &bp_of(C &c) { return c.bp; }
+template <typename T> auto &bp_of(flsgpu::host::ALPColumn<T> &c) { return c.ffor.bp; }
+}  // namespace detail
+
+// bindings::query_multi_column (kernel-bindings.cuh:30-35) and its host
+// harness kernels::host::query_multi_column (src/engine/multi-column-host-
+// kernels.cuh:13-123): ten device copies of the host column, each after the
+// bit widths were shuffled (data.cuh:521-531: a random permutation of the
+// widths, vector offsets recomputed as their prefix sum, so every copy is a
+// column of the same packed size), then the multi-column scan over the
+// first 1, 2, ..., 10 copies, n_samples times each with a device
+// synchronisation after every launch; the result is set when any of those
+// scans found a lane equal to magic_value in every column.  The shuffle
+// works on a copy of the widths (the reference permutes the caller's array
+// in place and keeps the old offsets).  Host column types: FFORColumn<u32 /
+// u64>, ALPColumn<float / double>.
+template <typename T, typename HostColumnT>
+bool query_multi_column(HostColumnT column, const unsigned unpack_n_vectors,
+                        const unsigned unpack_n_values, const enums::Unpacker unpacker,
+                        const enums::Patcher patcher, const T magic_value,
+                        const uint32_t n_samples) {
+  using DeviceColumnT = typename HostColumnT::DeviceColumnT;
+  constexpr int MAX_N_COLS = 10;
+  auto &bp = detail::bp_of(column);
+  const size_t nv = bp.get_n_vecs();
+  using UINT_T = typename flsgpu::detail::same_width_uint<T>::type;
+  constexpr size_t NL = 1024 / (8 * sizeof(UINT_T));
+  vbw_t *orig_bw = bp.bit_widths;
+  size_t *orig_offs = bp.vector_offsets;
+  vbw_t *bw = new vbw_t[nv ? nv : 1];
+  size_t *offs = new size_t[nv ? nv : 1];
+  std::memcpy(bw, orig_bw, nv);
+  std::random_device rd;
+  std::default_random_engine rng(rd());
+  DeviceColumnT dev[MAX_N_COLS];
+  for (int c = 0; c < MAX_N_COLS; ++c) {
+    std::shuffle(bw, bw + nv, rng);
+    size_t acc = 0;
+    for (size_t v = 0; v < nv; ++v) {
+      offs[v] = acc;
+      acc += (size_t)bw[v] * NL;
+    }
+    bp.bit_widths = bw;
+    bp.vector_offsets = offs;
+    dev[c] = column.copy_to_device();
+  }
+  bp.bit_widths = orig_bw;
+  bp.vector_offsets = orig_offs;
+  delete[] bw;
+  delete[] offs;
+  const auto o = detail::opts(unpack_n_vectors, unpack_n_values, unpacker, patcher);
+  detail::DeviceBuf<uint8_t> d(1);
+  flsgpu::detail::cuda_check(cudaMemset(d.p, 0, 1), "memset");
+  for (uint32_t n = 1; n <= (uint32_t)MAX_N_COLS; ++n)
+    for (uint32_t i = 0; i < n_samples; ++i) {
+      flsgpu::detail::check(detail::qmc(dev, n, magic_value, d.p, &o));
+      flsgpu::detail::cuda_check(cudaDeviceSynchronize(), "query_multi_column");
+    }
+  for (int c = 0; c < MAX_N_COLS; ++c) flsgpu::host::free_column(dev[c]);
   uint8_t h = 0;
   flsgpu::detail::cuda_check(cudaMemcpy(&h, d.p, 1, cudaMemcpyDeviceToHost), "copy");
   return h != 0;

@@ -284,6 +284,25 @@ def make_alprd_column(col: dict, n_values: int, dtype, device="cuda") -> DeviceC
     return DeviceColumn("alprd", "f64" if f64 else "f32", n_values, c, bufs, right.n_packed)
 
 
+def to_extended(col: DeviceColumn, stream=None) -> DeviceColumn:
+    """The lane-divided (ALPExtendedColumn) form of an ALP DeviceColumn,
+    converted on the GPU (flsgpu_alp_to_extended_*); shares the packed
+    words and metadata of `col`."""
+    torch = _torch()
+    f64 = col.dtype == "f64"
+    n_exc = int(col.c.n_exceptions)
+    dev = col.device
+    exc = torch.empty(max(n_exc, 1), dtype=torch.float64 if f64 else torch.float32, device=dev)
+    pos = torch.empty(max(n_exc, 1), dtype=torch.int16, device=dev)
+    oc = torch.empty(max(col.n_vecs * (16 if f64 else 32), 1), dtype=torch.int16, device=dev)
+    dst = ALPColumnC()
+    _check(_fn(f"flsgpu_alp_to_extended_{col.dtype}")(C.byref(col.c), P(_ptr(exc)), P(_ptr(pos)),
+                                                      P(_ptr(oc)), C.byref(dst),
+                                                      P(_stream_handle(stream))))
+    return DeviceColumn("alpx", col.dtype, col.n_values, dst,
+                        {"_exc": exc, "_pos": pos, "_oc": oc, "_base": col}, col.n_packed)
+
+
 def opts(unpacker: int = 18, patcher: int = 7, variant: int = VARIANT_AUTO,
          unpack_n_vectors: int = 1, unpack_n_values: int = 1, d_status=None,
          n_packed_values: int = 0) -> DecodeOpts:
