@@ -1010,6 +1010,9 @@ def main():
     ap.add_argument("--scale", type=float, default=1.0,
                     help="fraction of the benchmark column sizes (1.0 = full)")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--variant", type=int, default=0,
+                    help="decode kernel variant for the 64-bit-lane columns (0 = tuned default, "
+                         "1 register-rich, 2 register-capped, 3 staged)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extras", dest="extras", action="store_false",
                     help="ffor workload: only the headline FFOR decode (no fused-sum, ALP, "
@@ -1054,6 +1057,10 @@ def main():
     import torch
     rank, world, local = dist_init()
     dev = torch.device("cuda", torch.cuda.current_device())
+    if args.variant:
+        import flsgpu_b200 as F
+        F.tuning_set({"variant": {(t, k): args.variant for t in ("u64", "f64")
+                                  for k in (("bp", "ffor") if t == "u64" else ("alp", "alpx"))}})
     if args.tune or args.workload == "autotune":
         import flsgpu_b200 as F
         t0 = time.perf_counter()

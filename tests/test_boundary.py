@@ -98,8 +98,9 @@ def test_shim_query_multi_column(cuda, built):
     s = C.CDLL(str(built[0]))
     c = colgen.random_ffor(77, 20, 32, [0], base_max=4)
     c["bases"][:] = 3  # width 0: every value is 3
-    args = [_p(c["packed"]), C.c_size_t(c["packed"].size), _p(c["bit_widths"]),
-            _p(c["vector_offsets"].astype(np.uint64)), _p(c["bases"]), C.c_size_t(c["n_values"])]
+    offs = c["vector_offsets"].astype(np.uint64)
+    args = [_p(c["packed"]), C.c_size_t(c["packed"].size), _p(c["bit_widths"]), _p(offs),
+            _p(c["bases"]), C.c_size_t(c["n_values"])]
     found = C.c_int(-1)
     assert s.shim_query_multi_column_ffor_u32(*args, C.c_uint32(3), C.byref(found)) == 0
     assert found.value == 1
@@ -118,12 +119,17 @@ def test_shim_alp_decode_and_create_extended_column(cuda, built, f64, extended):
     n = n_vecs * 1024
     out = np.zeros(n, dt)
     fn = getattr(s, "shim_decompress_alp_" + ("f64" if f64 else "f32"))
-    rc = fn(_p(col["packed"].astype(ut)), C.c_size_t(col["packed"].size), _p(col["bit_widths"]),
-            _p(col["vector_offsets"].astype(np.uint64)), _p(col["bases"].astype(ut)),
-            C.c_size_t(n), _p(col["factor_indices"]), _p(col["fraction_indices"]),
-            C.c_size_t(col["exceptions"].size), _p(col["exceptions_offsets"].astype(np.uint64)),
-            _p(np.ascontiguousarray(col["exceptions"], dt)), _p(col["positions"]),
-            _p(col["counts"]), C.c_int(1 if extended else 0), _p(out))
+    # arrays converted once and kept alive across the call
+    a = {k: np.ascontiguousarray(col[k], t) for k, t in
+         (("packed", ut), ("bit_widths", np.uint8), ("vector_offsets", np.uint64), ("bases", ut),
+          ("factor_indices", np.uint8), ("fraction_indices", np.uint8),
+          ("exceptions_offsets", np.uint64), ("exceptions", dt), ("positions", np.uint16),
+          ("counts", np.uint16))}
+    rc = fn(_p(a["packed"]), C.c_size_t(a["packed"].size), _p(a["bit_widths"]),
+            _p(a["vector_offsets"]), _p(a["bases"]), C.c_size_t(n), _p(a["factor_indices"]),
+            _p(a["fraction_indices"]), C.c_size_t(a["exceptions"].size),
+            _p(a["exceptions_offsets"]), _p(a["exceptions"]), _p(a["positions"]),
+            _p(a["counts"]), C.c_int(1 if extended else 0), _p(out))
     assert rc == 0
     want = B.alp_decode(col, n_vecs, dt).view(ut)
     assert np.array_equal(out.view(ut), want)
