@@ -691,6 +691,57 @@ template <typename T> T *dalloc(size_t n, flsgpu_status &st) {
 
 }  // namespace
 
+namespace flsb200 {
+// A keyed permutation of [0, n): four Feistel rounds over 2 * half_bits
+// bits (a bijection of [0, 4^half_bits)), applied again while the result is
+// n or more (cycle walking; the domain is less than 4n, so few repeats, and
+// the walk ends within the cycle of x).
+__device__ __forceinline__ uint32_t mix32(uint32_t x) {
+  x ^= x >> 16;
+  x *= 0x7feb352dU;
+  x ^= x >> 15;
+  x *= 0x846ca68bU;
+  x ^= x >> 16;
+  return x;
+}
+__device__ __forceinline__ uint32_t permute_index(uint32_t i, uint32_t n, int half_bits,
+                                                  uint32_t key) {
+  const uint32_t mask = (1u << half_bits) - 1u;
+  const uint64_t domain = 1ull << (2 * half_bits);
+  uint32_t x = i;
+  for (uint64_t guard = 0; guard < domain; ++guard) {
+    uint32_t l = x >> half_bits, r = x & mask;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const uint32_t f = mix32(r ^ (key + 0x632BE5ABu * (uint32_t)k)) & mask;
+      const uint32_t nl = r;
+      r = l ^ f;
+      l = nl;
+    }
+    x = (l << half_bits) | r;
+    if (x < n) break;
+  }
+  return x;
+}
+
+// Row r of the epoch's training order is feature row permute_index(r):
+// 64 bf16 features (eight 16-byte chunks, one per thread) and the label.
+__global__ void __launch_bounds__(256) k_gather_rows(const __nv_bfloat16 *__restrict__ feat,
+                                                     const int16_t *__restrict__ labels,
+                                                     uint32_t n, size_t rows, int half_bits,
+                                                     uint32_t key, __nv_bfloat16 *out_feat,
+                                                     int16_t *out_lab) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= rows * 8) return;
+  const size_t r = i >> 3;
+  const int chunk = (int)(i & 7);
+  const uint32_t src = permute_index((uint32_t)r, n, half_bits, key);
+  reinterpret_cast<uint4 *>(out_feat)[r * 8 + chunk] =
+      reinterpret_cast<const uint4 *>(feat)[(size_t)src * 8 + chunk];
+  if (chunk == 0) out_lab[r] = labels[src];
+}
+}  // namespace flsb200
+
 struct flsgpu_alp_encoder {
   // parameters (fp32 master), Adam moments, gradients
   float *w = nullptr, *m = nullptr, *v = nullptr, *g = nullptr;
@@ -1108,34 +1159,24 @@ flsgpu_status flsgpu_alp_encoder_train(flsgpu_alp_encoder *e, const double *d_va
   if (!st) st = features(d_values, n_vecs, e->feat, s);
   if (!st) st = run_plain_labels(d_values, n_vecs, e->labels, nullptr, s);
   if (st) return st;
-  // shuffled copies of the rows per epoch are gathered on the host side
-  // from a permutation applied to the (small) feature and label arrays
-  std::vector<bf16> hf(n_vecs * kFeatures);
-  std::vector<int16_t> hl(n_vecs);
-  if ((st = check_cuda(cudaMemcpyAsync(hf.data(), e->feat, sizeof(bf16) * hf.size(), cudaMemcpyDeviceToHost, s), "copy")) ||
-      (st = check_cuda(cudaMemcpyAsync(hl.data(), e->labels, sizeof(int16_t) * hl.size(), cudaMemcpyDeviceToHost, s), "copy")) ||
-      (st = check_cuda(cudaStreamSynchronize(s), "sync")))
-    return st;
-  std::mt19937 rng(1234);
-  std::vector<size_t> perm(n_vecs);
-  for (size_t i = 0; i < n_vecs; ++i) perm[i] = i;
+  // every epoch visits the rows in a new order: a keyed permutation of the
+  // row indices, gathered into a batch-ordered copy on the device
   const size_t nb = n_vecs / batch;
   if (nb == 0) return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "fewer vectors than one batch");
-  std::vector<bf16> sf(nb * batch * kFeatures);
-  std::vector<int16_t> sl(nb * batch);
   bf16 *dfeat = nullptr;
   int16_t *dlab = nullptr;
-  st = check_cuda(cudaMalloc(&dfeat, sizeof(bf16) * sf.size()), "cudaMalloc");
-  if (!st) st = check_cuda(cudaMalloc(&dlab, sizeof(int16_t) * sl.size()), "cudaMalloc");
+  st = check_cuda(cudaMalloc(&dfeat, sizeof(bf16) * nb * batch * kFeatures), "cudaMalloc");
+  if (!st) st = check_cuda(cudaMalloc(&dlab, sizeof(int16_t) * nb * batch), "cudaMalloc");
+  int half_bits = 1;
+  while ((1ull << (2 * half_bits)) < n_vecs) ++half_bits;
   std::vector<float> lbuf(batch);
   for (uint32_t ep = 0; ep < epochs && !st; ++ep) {
-    std::shuffle(perm.begin(), perm.end(), rng);
-    for (size_t i = 0; i < nb * batch; ++i) {
-      std::memcpy(&sf[i * kFeatures], &hf[perm[i] * kFeatures], sizeof(bf16) * kFeatures);
-      sl[i] = hl[perm[i]];
-    }
-    st = check_cuda(cudaMemcpyAsync(dfeat, sf.data(), sizeof(bf16) * sf.size(), cudaMemcpyHostToDevice, s), "copy");
-    if (!st) st = check_cuda(cudaMemcpyAsync(dlab, sl.data(), sizeof(int16_t) * sl.size(), cudaMemcpyHostToDevice, s), "copy");
+    const uint32_t key = 0x9E3779B9u * (ep + 1) ^ 1234u;
+    const size_t rows = nb * batch;
+    k_gather_rows<<<(unsigned)((rows * 8 + 255) / 256), 256, 0, s>>>(
+        e->feat, e->labels, (uint32_t)n_vecs, rows, half_bits, key, dfeat, dlab);
+    note_launch();
+    st = check_cuda(cudaGetLastError(), "k_gather_rows");
     double eloss = 0;
     for (size_t b = 0; b < nb && !st; ++b) {
       st = forward_backward(e, dfeat + b * batch * kFeatures, dlab + b * batch, (int)batch, s);

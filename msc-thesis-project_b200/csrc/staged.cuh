@@ -9,11 +9,9 @@
 // on the slot's mbarrier) brings vector i + 1 into the other slot, and the
 // copy of vector i + 2 is issued as soon as vector i's slot is read.  The
 // unpack reads each value's one or two 32-bit stream words straight from
-// the slot.  A vector wider than 32 bits is copied when it is decoded, the
-// lines of each half-lane stream in turn (ceil(w / 2) <= 32 lines), into the
-// iteration's slot; a vector whose packed words are not 16-byte aligned is
-// copied there by the warp's own 8-byte loads.  Every unpack reads shared
-// memory, so the kernel needs few registers and three blocks fit per SM.
+// the slot.  Vectors wider than 32 bits, or with a packed-word address that
+// is not 16-byte aligned, take the register-held decode of k_store's
+// register-capped variant.
 //
 // Every wait on an mbarrier is bounded (about a second of SM clocks); a
 // wait that gives up raises FLSGPU_WAIT_TIMEOUT in the status word, waits
@@ -90,15 +88,10 @@ __device__ __forceinline__ void decode_words64(const uint32_t *base, int w, int 
       if constexpr (SMEM)
         return *q;
       else
-        return ld_stream_u32(q);  // asm volatile: stays within its group of 8
+        return __ldg(q);
     };
 #pragma unroll
     for (int k = 0; k < 32; ++k) {
-      // from global memory, loads are not hoisted across groups of 8
-      // values, so that few words are live at once
-      if constexpr (!SMEM) {
-        if ((k & 7) == 0 && k > 0) asm volatile("" ::: "memory");
-      }
       uint64_t v = 0;
       if (W > 0) {
         const int bit = k * W, j = bit >> 5, o = bit & 31;
@@ -142,69 +135,37 @@ __device__ __forceinline__ uint32_t first_exceptions(const ColumnParams &c, cons
 // One vector: decode (from the slot when s32 is given, else from global
 // memory), then patch its exceptions (ALP columns; p0 / e0 / ecnt from
 // first_exceptions); as store_one.
-// s32: the slot holding the vector's packed words (copied ahead), or null;
-// then `slot` (this iteration's, empty) is filled here, with bar / *phase
-// its barrier and parity.  False when a wait gave up.
 template <typename T, int KIND, int VAR>
-__device__ __forceinline__ bool store_one_staged(const KernelParams &p, size_t vi, const Meta<T> &m,
+__device__ __forceinline__ void store_one_staged(const KernelParams &p, size_t vi, const Meta<T> &m,
                                                  int t, const uint32_t *s32, uint32_t p0, T e0,
-                                                 uint32_t ecnt, unsigned char *slot, uint64_t *bar,
-                                                 uint32_t *phase) {
+                                                 uint32_t ecnt) {
   using U = typename UintOf<T>::U;
   using X = typename XformOf<T, KIND>::type;
   const ColumnParams &c = p.c;
   const U *vin;
   int w;
   X xf;
-  if (!setup_from_meta<T, KIND>(c, p.d_status, m, t, vin, w, xf)) return true;
+  if (!setup_from_meta<T, KIND>(c, p.d_status, m, t, vin, w, xf)) return;
   const size_t vbase = vi * VEC;
   const size_t rem = c.n_values - vbase;
   const int lim = rem < (size_t)VEC ? (int)rem : VEC;
   T *out = reinterpret_cast<T *>(p.out) + vbase;
   [[maybe_unused]] const bool pre =
       (KIND == K_ALP && c.patch && c.counts) || (KIND == K_ALPX && c.patch && c.oc);
-  auto put = [&](int idx, T v, auto pc) {
+  auto put_full = [&](int idx, T v, auto pc) { store_out<T, decltype(pc)::value>(out + idx, v); };
+  auto put_lim = [&](int idx, T v, auto pc) {
     if (idx < lim) store_out<T, decltype(pc)::value>(out + idx, v);
   };
-  // A vector not copied ahead (wider than 32 bits, or packed words not
-  // 16-byte aligned) is copied into this iteration's slot now, the lines of
-  // each half-lane stream in turn when it is wider than 32 bits.  One call
-  // site of the unpacker keeps the kernel's code (and registers) small.
-  const int half = t >> 4;
-  const char *src = reinterpret_cast<const char *>(vin);
-  const bool aligned = (reinterpret_cast<uintptr_t>(src) & 15u) == 0;
-  const int passes = (!s32 && w > kStageMaxW) ? 2 : 1;
-  for (int h = 0; h < passes; ++h) {
-    const uint32_t *b32 = s32;
-    if (!s32) {
-      const int l0 = (passes == 2 && h) ? (w >> 1) : 0;
-      const int nl = passes == 2 ? (w + 1) >> 1 : w;
-      if (h) {
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncwarp();
-      }
-      if (nl > 0) {
-        if (aligned) {
-          if (t == 0) bulk_to_slot(slot, src + (size_t)l0 * 128, (uint32_t)nl * 128u, bar);
-          const bool ok = __all_sync(0xffffffffu, mbar_wait(bar, *phase));
-          *phase ^= 1u;
-          if (!ok) {
-            if (t == 0) flag_status(p.d_status, FLSGPU_WAIT_TIMEOUT);
-            return false;
-          }
-        } else {
-          // 8-byte words, each thread a share of the lines
-          const uint64_t *s64 = reinterpret_cast<const uint64_t *>(src) + (size_t)l0 * 16;
-          uint64_t *d64 = reinterpret_cast<uint64_t *>(slot);
-          for (int i = t; i < nl * 16; i += 32) d64[i] = s64[i];
-          __syncwarp();
-        }
-      }
-      // the slot holds lines l0 .. l0 + nl - 1 of the vector
-      b32 = reinterpret_cast<const uint32_t *>(slot) - l0 * 32;
-    }
-    if (passes == 1 || half == h) decode_words64<true, VAR>(b32, w, t, xf, put);
-    __syncwarp();
+  if (s32) {
+    if (lim == VEC)
+      decode_words64<true, VAR>(s32, w, t, xf, put_full);
+    else
+      decode_words64<true, VAR>(s32, w, t, xf, put_lim);
+  } else {
+    if (lim == VEC)
+      decode_values<T, VAR>(vin, w, t, xf, put_full);
+    else
+      decode_values<T, VAR>(vin, w, t, xf, put_lim);
   }
   if constexpr (KIND == K_ALP || KIND == K_ALPX) {
     if (pre) {
@@ -221,7 +182,6 @@ __device__ __forceinline__ bool store_one_staged(const KernelParams &p, size_t v
         }
       }
       if (__any_sync(0xffffffffu, bad) && t == 0) flag_status(p.d_status, FLSGPU_BAD_EXCEPTION);
-      return true;
     } else if (c.patch) {
       __syncwarp();
       patch_vector<T, KIND>(c, p.d_status, vi, t, [&](int ps, T e) {
@@ -229,15 +189,13 @@ __device__ __forceinline__ bool store_one_staged(const KernelParams &p, size_t v
       });
     }
   }
-  return true;
 }
 
-// Whether vector metadata m can be copied into slots: width 1..64,
-// metadata that passes the checks, packed words 16-byte aligned.  Widths up
-// to 32 are copied one vector ahead; wider ones when they are decoded.
+// Whether vector metadata m is decoded from a slot: width 1..32, metadata
+// that passes the checks, packed words 16-byte aligned.
 template <typename T, int KIND>
-__device__ __forceinline__ bool slot_ok(const ColumnParams &c, const Meta<T> &m) {
-  if (m.w < 1 || m.w > 64) return false;
+__device__ __forceinline__ bool stageable(const ColumnParams &c, const Meta<T> &m) {
+  if (m.w < 1 || m.w > kStageMaxW) return false;
   if (c.n_packed && (m.off > c.n_packed || (size_t)m.w * 16 > c.n_packed - m.off)) return false;
   if constexpr (std::is_same<T, double>::value) {
     if (m.fi > 18 || m.ei > 20) return false;
@@ -245,13 +203,9 @@ __device__ __forceinline__ bool slot_ok(const ColumnParams &c, const Meta<T> &m)
   const uintptr_t src = reinterpret_cast<uintptr_t>(c.packed) + m.off * 8;
   return (src & 15u) == 0;
 }
-template <typename T, int KIND>
-__device__ __forceinline__ bool stageable(const ColumnParams &c, const Meta<T> &m) {
-  return m.w <= kStageMaxW && slot_ok<T, KIND>(c, m);
-}
 
 template <typename T, int KIND>
-__global__ void __launch_bounds__(256, 3) k_store_staged(const KernelParams p) {
+__global__ void __launch_bounds__(256, 2) k_store_staged(const KernelParams p) {
   static_assert(sizeof(T) == 8, "64-bit lanes only");
   constexpr int VAR = VAR_AUTO | VAR_OCC;
   extern __shared__ __align__(128) unsigned char st_smem[];
@@ -312,15 +266,7 @@ __global__ void __launch_bounds__(256, 3) k_store_staged(const KernelParams p) {
       phase ^= 1u << s;
       s32 = reinterpret_cast<const uint32_t *>(slot_base + s * kStageSlotBytes);
     }
-    // a vector not copied ahead uses this iteration's slot, empty then
-    uint32_t ph = (phase >> s) & 1u;
-    const bool ok = store_one_staged<T, KIND, VAR>(p, vi, m0, t, s32, cp, ce, cc,
-                                                   slot_base + s * kStageSlotBytes, &bars[s], &ph);
-    if (!st0) phase = (phase & ~(1u << s)) | (ph << s);
-    if (!ok) {
-      if (st1) mbar_wait(&bars[s ^ 1], (phase >> (s ^ 1)) & 1u);
-      return;
-    }
+    store_one_staged<T, KIND, VAR>(p, vi, m0, t, s32, cp, ce, cc);
     bool st2 = false;
     if (has2) {
       st2 = stageable<T, KIND>(c, m2);
