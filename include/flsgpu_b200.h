@@ -211,6 +211,19 @@ flsgpu_status flsgpu_decompress_ffor_u32(const flsgpu_ffor_column *column, uint3
                                          const flsgpu_decode_opts *opts, flsgpu_stream stream);
 flsgpu_status flsgpu_decompress_ffor_u64(const flsgpu_ffor_column *column, uint64_t *d_out,
                                          const flsgpu_decode_opts *opts, flsgpu_stream stream);
+/* 8- and 16-bit lanes (fls::unpack / fls::unffor for uint8_t / uint16_t,
+ * src/fls/fls-bindings.hpp:8-52, CPU-only in the reference): the same
+ * descriptors with packed_array holding u8 / u16 lane words (128 / 64 lanes
+ * per vector), vector_offsets in those words, bases u8 / u16; packed words
+ * and output 4-byte aligned. */
+flsgpu_status flsgpu_decompress_bp_u8(const flsgpu_bp_column *column, uint8_t *d_out,
+                                      const flsgpu_decode_opts *opts, flsgpu_stream stream);
+flsgpu_status flsgpu_decompress_bp_u16(const flsgpu_bp_column *column, uint16_t *d_out,
+                                       const flsgpu_decode_opts *opts, flsgpu_stream stream);
+flsgpu_status flsgpu_decompress_ffor_u8(const flsgpu_ffor_column *column, uint8_t *d_out,
+                                        const flsgpu_decode_opts *opts, flsgpu_stream stream);
+flsgpu_status flsgpu_decompress_ffor_u16(const flsgpu_ffor_column *column, uint16_t *d_out,
+                                         const flsgpu_decode_opts *opts, flsgpu_stream stream);
 flsgpu_status flsgpu_decompress_alp_f32(const flsgpu_alp_column *column, float *d_out,
                                         const flsgpu_decode_opts *opts, flsgpu_stream stream);
 flsgpu_status flsgpu_decompress_alp_f64(const flsgpu_alp_column *column, double *d_out,
@@ -264,6 +277,10 @@ flsgpu_status flsgpu_alp_to_extended_f64(const flsgpu_alp_column *src, double *d
 #define FLSGPU_BASE_MIN 0u
 #define FLSGPU_BASE_SIGNED_MIN 1u
 #define FLSGPU_BASE_ZERO 2u
+flsgpu_status flsgpu_ffor_encode_u8(const uint8_t *d_values, size_t n_values, uint32_t base_mode,
+                                    uint8_t *d_packed, uint8_t *d_bit_widths,
+                                    uint64_t *d_vector_offsets, uint8_t *d_bases,
+                                    uint64_t *d_n_packed, flsgpu_stream stream);
 flsgpu_status flsgpu_ffor_encode_u16(const uint16_t *d_values, size_t n_values, uint32_t base_mode,
                                      uint16_t *d_packed, uint8_t *d_bit_widths,
                                      uint64_t *d_vector_offsets, uint16_t *d_bases,

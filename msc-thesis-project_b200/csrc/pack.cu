@@ -15,7 +15,9 @@
 //        h*w .. h*w+w-1 of the lane's stream (the low / high halves of the
 //        64-bit words at packed[j*16 + l]);
 //   u16: thread t = lanes 2t and 2t+1, 16 values each (element lane + 64j);
-//        16-bit stream words 0..w-1 of each lane at packed[j*64 + lane].
+//        16-bit stream words 0..w-1 of each lane at packed[j*64 + lane];
+//   u8:  thread t = lanes 4t .. 4t+3, 8 values each (element lane + 128j);
+//        8-bit stream words 0..w-1 of each lane at packed[j*128 + lane].
 // A value occupies bits [k*w, (k+1)*w) of its lane's stream, least
 // significant bit first, so the words decode with flsgpu_decompress_*.
 #include "common.cuh"
@@ -28,8 +30,10 @@ template <typename U> __device__ __forceinline__ size_t owned_index(int t, int k
     return (size_t)t + 32u * k;
   } else if constexpr (sizeof(U) == 8) {
     return (size_t)(t & 15) + 16u * (32u * (t >> 4) + k);
-  } else {
+  } else if constexpr (sizeof(U) == 2) {
     return (size_t)(2 * t + (k >> 4)) + 64u * (k & 15);
+  } else {
+    return (size_t)(4 * t + (k >> 3)) + 128u * (k & 7);
   }
 }
 
@@ -153,12 +157,20 @@ __global__ void __launch_bounds__(256) k_pack_write(const U *__restrict__ vals, 
           bwr.put(d >> 32, w - 32, emit);
         }
       }
-    } else {
+    } else if constexpr (sizeof(U) == 2) {
       for (int half = 0; half < 2; ++half) {
         const int lane = 2 * t + half;
         BitWriter<16> bwr;
         auto emit = [&](int i, uint32_t x) { out[(size_t)i * 64 + lane] = (U)x; };
         for (int j = 0; j < 16; ++j) bwr.put((uint16_t)(vec[(size_t)lane + 64u * j] - base), w, emit);
+      }
+    } else {
+      // u8: thread t = lanes 4t .. 4t + 3, 8 values each (element lane + 128 j)
+      for (int q = 0; q < 4; ++q) {
+        const int lane = 4 * t + q;
+        BitWriter<8> bwr;
+        auto emit = [&](int i, uint32_t x) { out[(size_t)i * 128 + lane] = (U)x; };
+        for (int j = 0; j < 8; ++j) bwr.put((uint8_t)(vec[(size_t)lane + 128u * j] - base), w, emit);
       }
     }
   }
@@ -188,6 +200,13 @@ static flsgpu_status pack_column(const U *vals, size_t n_values, uint32_t mode, 
 using namespace flsb200;
 
 extern "C" {
+flsgpu_status flsgpu_ffor_encode_u8(const uint8_t *d_values, size_t n_values, uint32_t base_mode,
+                                    uint8_t *d_packed, uint8_t *d_bit_widths,
+                                    uint64_t *d_vector_offsets, uint8_t *d_bases,
+                                    uint64_t *d_n_packed, flsgpu_stream stream) {
+  return pack_column<uint8_t>(d_values, n_values, base_mode, d_packed, d_bit_widths,
+                              d_vector_offsets, d_bases, d_n_packed, stream);
+}
 flsgpu_status flsgpu_ffor_encode_u16(const uint16_t *d_values, size_t n_values, uint32_t base_mode,
                                      uint16_t *d_packed, uint8_t *d_bit_widths,
                                      uint64_t *d_vector_offsets, uint16_t *d_bases,

@@ -143,7 +143,8 @@ def _dev(a: np.ndarray, device):
     return t.to(device)
 
 
-TORCH_OF_BITS = {"u32": "int32", "u64": "int64", "f32": "float32", "f64": "float64"}
+TORCH_OF_BITS = {"u8": "uint8", "u16": "int16", "u32": "int32", "u64": "int64", "f32": "float32",
+                 "f64": "float64"}
 
 
 @dataclass
@@ -177,7 +178,10 @@ class DeviceColumn:
 
 def make_ffor_column(packed: np.ndarray, bit_widths: np.ndarray, offsets: np.ndarray,
                      bases: np.ndarray | None, n_values: int, device="cuda") -> DeviceColumn:
-    dt = "u64" if packed.dtype == np.uint64 else "u32"
+    dt = {np.dtype(np.uint64): "u64", np.dtype(np.uint32): "u32", np.dtype(np.uint16): "u16",
+          np.dtype(np.uint8): "u8"}[np.dtype(packed.dtype)]
+    if dt in ("u8", "u16") and packed.size % (4 // packed.itemsize):
+        packed = np.concatenate([packed, np.zeros(4 // packed.itemsize - packed.size % (4 // packed.itemsize), packed.dtype)])
     bufs = {"packed": _dev(packed if packed.size else np.zeros(1, packed.dtype), device),
             "bit_widths": _dev(bit_widths.astype(np.uint8), device),
             "vector_offsets": _dev(offsets.astype(np.uint64), device)}
@@ -196,11 +200,9 @@ BASE_MIN, BASE_SIGNED_MIN, BASE_ZERO = 0, 1, 2
 
 def ffor_encode(values, base_mode: int = BASE_MIN, stream=None):
     """FastLanes FFOR / BP packing on the GPU (flsgpu_ffor_encode_*) of a
-    device tensor of int16 / int32 / int64 (read as u16 / u32 / u64),
-    values.numel() % 1024 == 0.  Returns a DeviceColumn ("ffor", or "bp" for
-    BASE_ZERO) for 32- and 64-bit values, and a dict of the packed arrays for
-    16-bit values (ALP-RD left parts).  Synchronises to read the packed
-    size."""
+    device tensor of uint8 / int16 / int32 / int64 (read as u8 / u16 / u32 /
+    u64), values.numel() % 1024 == 0.  Returns a DeviceColumn ("ffor", or
+    "bp" for BASE_ZERO).  Synchronises to read the packed size."""
     torch = _torch()
     n = values.numel()
     bits = values.element_size() * 8
@@ -218,10 +220,6 @@ def ffor_encode(values, base_mode: int = BASE_MIN, stream=None):
     n_packed = int(total.item())
     bufs = {"packed": packed[:n_packed], "bit_widths": bw[:n_vecs], "vector_offsets": offs[:n_vecs],
             "_keep": packed}
-    if bits == 16:
-        bufs["bases"] = bases[:n_vecs]
-        bufs["n_packed"] = n_packed
-        return bufs
     bp = BPColumnC(n, n_vecs, _ptr(packed), _ptr(bw), _ptr(offs))
     if base_mode == BASE_ZERO:
         return DeviceColumn("bp", f"u{bits}", n, bp, bufs, n_packed)

@@ -58,6 +58,9 @@ class RDState(C.Structure):
 
 
 _ORACLE_SIGS = {
+    "orc_pack_u8": (None, [P, P, I]), "orc_unpack_u8": (None, [P, P, I]),
+    "orc_ffor_u8": (None, [P, P, I, C.c_uint8]), "orc_ffor_u16": (None, [P, P, I, U16]),
+    "orc_unffor_u8": (None, [P, P, I, C.c_uint8]), "orc_unffor_u16": (None, [P, P, I, U16]),
     "orc_pack_u16": (None, [P, P, I]), "orc_pack_u32": (None, [P, P, I]),
     "orc_pack_u64": (None, [P, P, I]), "orc_unpack_u16": (None, [P, P, I]),
     "orc_unpack_u32": (None, [P, P, I]), "orc_unpack_u64": (None, [P, P, I]),
@@ -95,6 +98,9 @@ _ORACLE_SIGS = {
 }
 
 _REF_SIGS = {
+    "ref_pack_u8": (None, [P, P, I]), "ref_unpack_u8": (None, [P, P, I]),
+    "ref_ffor_u8": (None, [P, P, I, C.c_uint8]), "ref_ffor_u16": (None, [P, P, I, U16]),
+    "ref_unffor_u8": (None, [P, P, I, C.c_uint8]), "ref_unffor_u16": (None, [P, P, I, U16]),
     "ref_pack_u16": (None, [P, P, I]), "ref_pack_u32": (None, [P, P, I]),
     "ref_pack_u64": (None, [P, P, I]), "ref_unpack_u16": (None, [P, P, I]),
     "ref_unpack_u32": (None, [P, P, I]), "ref_unpack_u64": (None, [P, P, I]),

@@ -65,12 +65,31 @@ static inline uint64_t mask_bits(int bw) {
     }                                                                        \
   }
 
+DEFINE_FLS(8, uint8_t)
 DEFINE_FLS(16, uint16_t)
 DEFINE_FLS(32, uint32_t)
 DEFINE_FLS(64, uint64_t)
 
 /* fls::ffor packs (in - base) (src/fls/ffor.cpp:29861); fls::unffor adds
  * the base back with unsigned wraparound (src/fls/unffor.cpp:22901). */
+void orc_ffor_u8(const uint8_t *in, uint8_t *out, int bw, uint8_t base) {
+  uint8_t tmp[VEC];
+  for (int i = 0; i < VEC; ++i) tmp[i] = (uint8_t)(in[i] - base);
+  orc_pack_u8(tmp, out, bw);
+}
+void orc_ffor_u16(const uint16_t *in, uint16_t *out, int bw, uint16_t base) {
+  uint16_t tmp[VEC];
+  for (int i = 0; i < VEC; ++i) tmp[i] = (uint16_t)(in[i] - base);
+  orc_pack_u16(tmp, out, bw);
+}
+void orc_unffor_u8(const uint8_t *in, uint8_t *out, int bw, uint8_t base) {
+  orc_unpack_u8(in, out, bw);
+  for (int i = 0; i < VEC; ++i) out[i] = (uint8_t)(out[i] + base);
+}
+void orc_unffor_u16(const uint16_t *in, uint16_t *out, int bw, uint16_t base) {
+  orc_unpack_u16(in, out, bw);
+  for (int i = 0; i < VEC; ++i) out[i] = (uint16_t)(out[i] + base);
+}
 void orc_ffor_u32(const uint32_t *in, uint32_t *out, int bw, uint32_t base) {
   uint32_t tmp[VEC];
   for (int i = 0; i < VEC; ++i) tmp[i] = in[i] - base;

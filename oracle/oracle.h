@@ -29,6 +29,12 @@ void orc_pack_u64(const uint64_t *in, uint64_t *out, int bw);
 void orc_unpack_u16(const uint16_t *in, uint16_t *out, int bw);
 void orc_unpack_u32(const uint32_t *in, uint32_t *out, int bw);
 void orc_unpack_u64(const uint64_t *in, uint64_t *out, int bw);
+void orc_pack_u8(const uint8_t *in, uint8_t *out, int bw);
+void orc_unpack_u8(const uint8_t *in, uint8_t *out, int bw);
+void orc_ffor_u8(const uint8_t *in, uint8_t *out, int bw, uint8_t base);
+void orc_ffor_u16(const uint16_t *in, uint16_t *out, int bw, uint16_t base);
+void orc_unffor_u8(const uint8_t *in, uint8_t *out, int bw, uint8_t base);
+void orc_unffor_u16(const uint16_t *in, uint16_t *out, int bw, uint16_t base);
 void orc_ffor_u32(const uint32_t *in, uint32_t *out, int bw, uint32_t base);
 void orc_ffor_u64(const uint64_t *in, uint64_t *out, int bw, uint64_t base);
 void orc_unffor_u32(const uint32_t *in, uint32_t *out, int bw, uint32_t base);

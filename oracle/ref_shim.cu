@@ -27,6 +27,12 @@ extern "C" void ref_pack_u64(const uint64_t *in, uint64_t *out, int bw) { fls::p
 extern "C" void ref_unpack_u16(const uint16_t *in, uint16_t *out, int bw) { fls::unpack(in, out, (uint8_t)bw); }
 extern "C" void ref_unpack_u32(const uint32_t *in, uint32_t *out, int bw) { fls::unpack(in, out, (uint8_t)bw); }
 extern "C" void ref_unpack_u64(const uint64_t *in, uint64_t *out, int bw) { fls::unpack(in, out, (uint8_t)bw); }
+extern "C" void ref_pack_u8(const uint8_t *in, uint8_t *out, int bw) { fls::pack(in, out, (uint8_t)bw); }
+extern "C" void ref_unpack_u8(const uint8_t *in, uint8_t *out, int bw) { fls::unpack(in, out, (uint8_t)bw); }
+extern "C" void ref_ffor_u8(const uint8_t *in, uint8_t *out, int bw, uint8_t base) { fls::ffor(in, out, (uint8_t)bw, &base); }
+extern "C" void ref_ffor_u16(const uint16_t *in, uint16_t *out, int bw, uint16_t base) { fls::ffor(in, out, (uint8_t)bw, &base); }
+extern "C" void ref_unffor_u8(const uint8_t *in, uint8_t *out, int bw, uint8_t base) { fls::unffor(in, out, (uint8_t)bw, &base); }
+extern "C" void ref_unffor_u16(const uint16_t *in, uint16_t *out, int bw, uint16_t base) { fls::unffor(in, out, (uint8_t)bw, &base); }
 extern "C" void ref_ffor_u32(const uint32_t *in, uint32_t *out, int bw, uint32_t base) { fls::ffor(in, out, (uint8_t)bw, &base); }
 extern "C" void ref_ffor_u64(const uint64_t *in, uint64_t *out, int bw, uint64_t base) { fls::ffor(in, out, (uint8_t)bw, &base); }
 extern "C" void ref_unffor_u32(const uint32_t *in, uint32_t *out, int bw, uint32_t base) { fls::unffor(in, out, (uint8_t)bw, &base); }

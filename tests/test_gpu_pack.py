@@ -11,8 +11,8 @@ from oracle import binding as B
 
 pytestmark = pytest.mark.gpu
 
-UT = {16: np.uint16, 32: np.uint32, 64: np.uint64}
-ST = {16: np.int16, 32: np.int32, 64: np.int64}
+UT = {8: np.uint8, 16: np.uint16, 32: np.uint32, 64: np.uint64}
+ST = {8: np.uint8, 16: np.int16, 32: np.int32, 64: np.int64}
 
 
 def _values(rng, bits, n_vecs, widths, signed=False, zero_base=False):
@@ -112,7 +112,7 @@ def test_bp_encode_u16_matches_oracle(cuda):
     r, packed, bw, offs, _ = _run(cuda, vals, 16, F.BASE_ZERO)
     assert np.array_equal(bw, want_bw)
     assert np.array_equal(packed, want_packed)
-    assert r["n_packed"] == want_packed.size
+    assert r.n_packed == want_packed.size
 
 
 def test_ffor_encode_edges(cuda):

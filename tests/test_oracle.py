@@ -129,3 +129,32 @@ def test_full_width_falp_quirk_is_known():
     r.ref_falp_f64(B.ptr(packed), B.ptr(a), 64, 3, 2, 5)
     ORC.orc_falp_f64(B.ptr(packed), B.ptr(b), 64, 3, 2, 5)
     assert not np.array_equal(a.view(np.uint64), b.view(np.uint64))
+
+
+@needs_ref
+@pytest.mark.parametrize("bits", [8, 16])
+def test_small_widths_pack_ffor_against_reference(bits):
+    """u8 / u16 FastLanes (fls::pack / unpack / ffor / unffor,
+    src/fls/fls-bindings.hpp:8-52) at every width: the oracle writes the
+    reference's words and decodes its words."""
+    r = B.ref()
+    ut = np.uint8 if bits == 8 else np.uint16
+    rng = np.random.default_rng(bits)
+    for w in range(bits + 1):
+        base = int(rng.integers(0, 2 ** bits))
+        vals = ((rng.integers(0, 2 ** w, 1024) + base) % 2 ** bits).astype(ut)
+        raw = rng.integers(0, 2 ** w, 1024).astype(ut)
+        for fn_pack, args in ((f"pack_u{bits}", (raw,)), (f"ffor_u{bits}", (vals, base))):
+            a = np.zeros(1024, ut)
+            b = np.zeros(1024, ut)
+            getattr(r, "ref_" + fn_pack)(B.ptr(args[0]), B.ptr(a), w, *args[1:])
+            getattr(ORC, "orc_" + fn_pack)(B.ptr(args[0]), B.ptr(b), w, *args[1:])
+            n = w * (1024 // bits)
+            assert np.array_equal(a[:n], b[:n]), (fn_pack, w)
+        packed = rng.integers(0, 2 ** bits, 1024).astype(ut)
+        for fn, extra in ((f"unpack_u{bits}", ()), (f"unffor_u{bits}", (base,))):
+            a = np.zeros(1024, ut)
+            b = np.zeros(1024, ut)
+            getattr(r, "ref_" + fn)(B.ptr(packed), B.ptr(a), w, *extra)
+            getattr(ORC, "orc_" + fn)(B.ptr(packed), B.ptr(b), w, *extra)
+            assert np.array_equal(a, b), (fn, w)
