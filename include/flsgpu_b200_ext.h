@@ -203,6 +203,18 @@ flsgpu_status flsgpu_alp_encoder_gradients(flsgpu_alp_encoder *encoder, const vo
                                            float *h_loss, flsgpu_stream stream);
 flsgpu_status flsgpu_alp_encoder_save(const flsgpu_alp_encoder *encoder, const char *path);
 flsgpu_status flsgpu_alp_encoder_load(flsgpu_alp_encoder *encoder, const char *path);
+/* The f32 GPU encoder: the float path of alp::encode (encoder.hpp:302-379,
+ * alp-bindings.cu:84-206) with the pair chosen per vector by the plain
+ * search (the 66 pairs 0 <= f <= e <= 10 on the vector's 32 samples, the
+ * estimate and tie rules of find_top_k_combinations), exceptions and fill
+ * of encode_simdized, FFOR at the signed minimum; an ALPColumn<float> in
+ * the encoder's workspace (valid until its next encode).  n_rd counts the
+ * vectors whose estimate reaches the ALP-RD limit (encoded as ALP all the
+ * same).  Synchronises. */
+flsgpu_status flsgpu_alp_encode_f32(flsgpu_alp_encoder *encoder, const float *d_values,
+                                    size_t n_values, flsgpu_alp_encode_result *out,
+                                    flsgpu_stream stream);
+
 /* Hybrid encode: as flsgpu_alp_encode_f64, but the vectors that call for
  * ALP-RD are encoded as ALP-RD (upstream ALP switches scheme there,
  * src/alp/encoder.hpp:208-211, where the reference's alp::encode gives up)

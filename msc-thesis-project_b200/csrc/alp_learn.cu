@@ -766,6 +766,9 @@ struct flsgpu_alp_encoder {
   size_t *exc_offs = nullptr, *vec_offs = nullptr;
   // ALP-RD encoder workspace (its column, and the RD part of hybrid columns)
   RDWork rd;
+  // f32 encoder: per-vector sizes and offsets ([2][cap_vecs]), scan blocks
+  uint32_t *f32_sizes = nullptr;
+  size_t *f32_offs = nullptr, *f32_blk = nullptr, *f32_tot = nullptr;
 };
 
 namespace {
@@ -805,8 +808,11 @@ void free_enc(flsgpu_alp_encoder *e) {
                   (void *)e->sl.bw, (void *)e->sl.base,
                   (void *)e->sl.fac, (void *)e->sl.exp, (void *)e->sl.count, (void *)e->sl.flags,
                   (void *)e->off_words, (void *)e->off_exc, (void *)e->totals, (void *)e->packed,
-                  (void *)e->exc, (void *)e->pos})
+                  (void *)e->exc, (void *)e->pos, (void *)e->f32_sizes, (void *)e->f32_offs,
+                  (void *)e->f32_blk, (void *)e->f32_tot})
     if (p) cudaFree(p);
+  e->f32_sizes = nullptr;
+  e->f32_offs = e->f32_blk = e->f32_tot = nullptr;
   e->feat = nullptr;
   e->labels = e->cand = nullptr;
   e->sl = EncodeSlots{};
@@ -843,6 +849,10 @@ flsgpu_status ensure_vecs(flsgpu_alp_encoder *e, size_t n_vecs) {
   e->packed = dalloc<uint64_t>(n * VEC, st);
   e->exc = dalloc<double>(n * VEC, st);
   e->pos = dalloc<uint16_t>(n * VEC, st);
+  e->f32_sizes = dalloc<uint32_t>(2 * n, st);
+  e->f32_offs = dalloc<size_t>(2 * n, st);
+  e->f32_blk = dalloc<size_t>(2 * (n / 1024 + 1), st);
+  e->f32_tot = dalloc<size_t>(4, st);
   if (st == FLSGPU_OK) e->cap_vecs = n;
   return st;
 }
@@ -1394,6 +1404,66 @@ flsgpu_status flsgpu_alp_encode_hybrid_f64(flsgpu_alp_encoder *e, const double *
   // scheme byte per vector
   out->compressed_bytes = tot[0] * 8 + tot[1] * 10 + n_alp * 11 + rtot[0] * 8 + rtot[1] * 2 +
                           rtot[2] * 4 + n_rd * 48 + n_vecs;
+  return FLSGPU_OK;
+}
+
+flsgpu_status flsgpu_alp_encode_f32(flsgpu_alp_encoder *e, const float *d_values,
+                                    size_t n_values, flsgpu_alp_encode_result *out,
+                                    flsgpu_stream stream) {
+  if (!e || !d_values || !out || (n_values % VEC))
+    return set_error(FLSGPU_ERR_INVALID_ARGUMENT, "f32 encode: bad arguments");
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t n_vecs = n_values / VEC;
+  flsgpu_status st = ensure_vecs(e, n_vecs);
+  if (st) return st;
+  const size_t stride = e->cap_vecs, bstride = e->cap_vecs / 1024 + 1;
+  Enc32Slots sl{};
+  sl.bw = e->sl.bw;
+  sl.fac = e->sl.fac;
+  sl.exp = e->sl.exp;
+  sl.base = reinterpret_cast<uint32_t *>(e->sl.base);
+  sl.fill = reinterpret_cast<int32_t *>(e->sl.fill);
+  sl.count = e->sl.count;
+  sl.exc_mask = e->sl.exc_mask;
+  sl.sizes = e->f32_sizes;
+  sl.stride = stride;
+  sl.n_rd = e->f32_tot + 2;
+  uint32_t *packed = reinterpret_cast<uint32_t *>(e->packed);
+  float *exc = reinterpret_cast<float *>(e->exc);
+  size_t tot[3] = {0, 0, 0};
+  if (n_vecs &&
+      ((st = check_cuda(cudaMemsetAsync(e->f32_tot + 2, 0, sizeof(size_t), s), "memset")) ||
+       (st = run_alp_encode_f32(d_values, n_vecs, sl, e->f32_offs, e->f32_blk, bstride,
+                                e->f32_tot, packed, exc, e->pos, s)) ||
+       (st = check_cuda(cudaMemcpyAsync(tot, e->f32_tot, sizeof(tot), cudaMemcpyDeviceToHost, s),
+                        "copy")) ||
+       (st = check_cuda(cudaStreamSynchronize(s), "sync"))))
+    return st;
+  std::memset(out, 0, sizeof(*out));
+  flsgpu_alp_column &c = out->column;
+  c.n_values = n_values;
+  c.ffor.n_values = n_values;
+  c.ffor.bp.n_values = n_values;
+  c.ffor.bp.n_vecs = n_vecs;
+  c.ffor.bp.packed_array = packed;
+  c.ffor.bp.bit_widths = sl.bw;
+  c.ffor.bp.vector_offsets = e->f32_offs;
+  c.ffor.bases = sl.base;
+  c.factor_indices = sl.fac;
+  c.fraction_indices = sl.exp;
+  c.n_exceptions = tot[1];
+  c.exceptions_offsets = e->f32_offs + stride;
+  c.exceptions = exc;
+  c.positions = e->pos;
+  c.counts = sl.count;
+  out->n_packed_words = tot[0];
+  out->n_exceptions = tot[1];
+  // reference accounting (alp-bindings.cu:19-43): packed bytes, 6 B per
+  // exception (value + position), 3 + 4 B of per-vector metadata
+  out->compressed_bytes = tot[0] * 4 + tot[1] * 6 + n_vecs * 7;
+  out->n_fallback = 0;
+  out->n_rd = tot[2];
+  out->mean_bit_width = 0.0;
   return FLSGPU_OK;
 }
 

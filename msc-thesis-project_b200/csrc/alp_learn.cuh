@@ -61,6 +61,23 @@ flsgpu_status run_alp_encode(const double *vals, size_t n_vecs, int mode, const 
                              size_t *off_exc, size_t *totals, uint64_t *packed, double *exc,
                              uint16_t *pos, cudaStream_t s, RDWork *rd = nullptr);
 
+// The f32 encoder (alp_encode_f32.cu): per-vector parameters and sizes.
+struct Enc32Slots {
+  uint8_t *bw, *fac, *exp;
+  uint32_t *base;
+  int32_t *fill;
+  uint16_t *count;
+  uint32_t *exc_mask;   // per vector, 32 words: thread t's exception bits
+  uint32_t *sizes;      // [2][stride]: packed words, exceptions
+  size_t stride;
+  size_t *n_rd;         // vectors whose estimate reaches the ALP-RD limit
+                        // (encoded as ALP all the same; counted)
+};
+
+flsgpu_status run_alp_encode_f32(const float *vals, size_t n_vecs, const Enc32Slots &sl,
+                                 size_t *offs, size_t *blk, size_t bstride, size_t *totals,
+                                 uint32_t *packed, float *exc, uint16_t *pos, cudaStream_t s);
+
 struct GemmArgs {
   const __nv_bfloat16 *A;
   const __nv_bfloat16 *B;

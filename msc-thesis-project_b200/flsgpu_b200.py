@@ -763,6 +763,14 @@ class AlpEncoder:
                                            P(_stream_handle(stream))))
         return r
 
+    def encode_f32(self, values, stream=None) -> EncodeResultC:
+        """ALP encode of an f32 column (float32 tensor) with the plain
+        per-vector search; decodes with encoded_column(..., dtype="f32")."""
+        r = EncodeResultC()
+        _check(_fn("flsgpu_alp_encode_f32")(self.h, P(_ptr(values)), SZ(values.numel()),
+                                           C.byref(r), P(_stream_handle(stream))))
+        return r
+
     def encode_hybrid(self, values, mode: int, stream=None) -> HybridEncodeResultC:
         """Hybrid ALP / ALP-RD encode of an f64 column (mode 0 plain search,
         1 learned proposal); ALP-RD vectors get a dictionary of their own."""
@@ -829,10 +837,10 @@ class AlpEncoder:
             self.h = None
 
 
-def encoded_column(res: EncodeResultC, n_values: int, keep=None) -> DeviceColumn:
+def encoded_column(res: EncodeResultC, n_values: int, keep=None, dtype: str = "f64") -> DeviceColumn:
     """The encoder's output as a decodable DeviceColumn (device arrays owned
     by the encoder; valid until its next encode)."""
-    return DeviceColumn("alp", "f64", n_values, res.column, {"_owner": keep} if keep else {},
+    return DeviceColumn("alp", dtype, n_values, res.column, {"_owner": keep} if keep else {},
                         int(res.n_packed_words))
 
 

@@ -58,6 +58,8 @@ class RDState(C.Structure):
 
 
 _ORACLE_SIGS = {
+    "orc_alp_vector_best_f32": (I, [P, P]),
+    "orc_alp_encode_vector_f32": (I, [P, I, I, P, P, P]),
     "orc_pack_u8": (None, [P, P, I]), "orc_unpack_u8": (None, [P, P, I]),
     "orc_ffor_u8": (None, [P, P, I, C.c_uint8]), "orc_ffor_u16": (None, [P, P, I, U16]),
     "orc_unffor_u8": (None, [P, P, I, C.c_uint8]), "orc_unffor_u16": (None, [P, P, I, U16]),

@@ -490,6 +490,20 @@ int orc_alp_vector_best_f64(const double *vec, uint64_t *est_bits) {
   return ke[0] * 32 + kf[0];
 }
 
+int orc_alp_vector_best_f32(const float *vec, uint64_t *est_bits) {
+  float smp[32];
+  for (int i = 0; i < 32; ++i) smp[i] = vec[i * 32];
+  uint8_t ke[5], kf[5];
+  uint64_t best = 0;
+  const int saved = g_rd_as_alp;
+  g_rd_as_alp = 1; /* the pair is wanted even where ALP-RD would be chosen */
+  const int k = topk_from_sample_f32(smp, 32, ke, kf, &best);
+  g_rd_as_alp = saved;
+  if (est_bits) *est_bits = best;
+  if (k <= 0) return -1;
+  return ke[0] * 32 + kf[0];
+}
+
 /* find_best_exponent_factor_from_combinations, encoder.hpp:237-300 */
 #define DEFINE_CHOOSE(SUF, PT, ST, UT, EXCBITS, CB)                          \
   static void choose_##SUF(const PT *vec, int k, const uint8_t *ke,         \
@@ -584,6 +598,10 @@ DEFINE_ENCVEC(f32, float, int32_t, uint32_t, 0x7FFFFFFFU, 0x7F800000U,
 int orc_alp_encode_vector_f64(const double *vec, int exp, int fac,
                               int64_t *encoded, double *exc, uint16_t *pos) {
   return encode_vector_f64(vec, exp, fac, encoded, exc, pos);
+}
+int orc_alp_encode_vector_f32(const float *vec, int exp, int fac, int32_t *encoded, float *exc,
+                              uint16_t *pos) {
+  return encode_vector_f32(vec, exp, fac, encoded, exc, pos);
 }
 
 /* alp::encode, src/alp/alp-bindings.cu:84-206: per vector, second-level

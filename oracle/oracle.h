@@ -122,6 +122,11 @@ void orc_set_rd_as_alp(int on);
  * no pair has >= 2 non-exceptions or the estimate crosses the RD limit.
  * est_bits receives the estimated sample bits of the chosen pair. */
 int orc_alp_vector_best_f64(const double *vec, uint64_t *est_bits);
+/* f32: the best pair of the vector's 32 samples (returned even where the
+ * estimate reaches the ALP-RD limit), e*32+f; and one vector's encode. */
+int orc_alp_vector_best_f32(const float *vec, uint64_t *est_bits);
+int orc_alp_encode_vector_f32(const float *vec, int exp, int fac, int32_t *encoded, float *exc,
+                              uint16_t *pos);
 /* second-level choice for one vector among k candidates */
 void orc_alp_vector_choose_f64(const double *vec, int k, const uint8_t *k_exp,
                                const uint8_t *k_fac, uint8_t *exp,
