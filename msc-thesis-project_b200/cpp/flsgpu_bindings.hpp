@@ -26,10 +26,12 @@
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
+#include <fstream>
 #include <random>
 #include <stdexcept>
 #include <string>
 #include <type_traits>
+#include <utility>
 
 #include "../../include/flsgpu_b200.h"
 
@@ -293,6 +295,44 @@ template <typename T> void free_column(device::ALPExtendedColumn<T> c) {
 }
 }  // namespace host
 }  // namespace flsgpu
+
+namespace data {
+namespace arrays {
+// data::arrays::read_file_as (src/engine/data.cuh:184-232): a binary file of
+// T values as a host column of `input_count` values (0: the whole file),
+// rounded down to whole vectors of 1024; when the file holds fewer values
+// than asked for, its values are repeated until the column is full.  The
+// array is new T[count] (release with delete[]).  Throws
+// std::invalid_argument when the file cannot be opened or read, when its
+// size is not a multiple of sizeof(T), or when it is empty but values are
+// asked for (where the reference would loop forever).
+template <typename T>
+std::pair<T *, size_t> read_file_as(const std::string path, const size_t input_count) {
+  std::ifstream f(path, std::ios::binary | std::ios::ate);
+  if (!f) throw std::invalid_argument("could not open " + path);
+  const std::streamsize file_size = f.tellg();
+  f.seekg(0, std::ios::beg);
+  if ((size_t)file_size % sizeof(T) != 0)
+    throw std::invalid_argument("file size is not a multiple of the value size");
+  const size_t in_file = (size_t)file_size / sizeof(T);
+  size_t count = input_count == 0 ? in_file : input_count;
+  count -= count % 1024;
+  if (count && !in_file) throw std::invalid_argument("empty file");
+  T *column = new T[count ? count : 1];
+  const size_t n_read = in_file < count ? in_file : count;
+  if (n_read && !f.read(reinterpret_cast<char *>(column), (std::streamsize)(n_read * sizeof(T)))) {
+    delete[] column;
+    throw std::invalid_argument("failed to read " + path);
+  }
+  for (size_t filled = n_read; filled < count;) {
+    const size_t n = (count - filled) < in_file ? (count - filled) : in_file;
+    std::memcpy(column + filled, column, n * sizeof(T));
+    filled += n;
+  }
+  return std::make_pair(column, count);
+}
+}  // namespace arrays
+}  // namespace data
 
 namespace bindings {
 namespace detail {

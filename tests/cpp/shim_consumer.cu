@@ -97,6 +97,15 @@ extern "C" {
 FFOR_DECODE(u32, uint32_t)
 FFOR_DECODE(u64, uint64_t)
 
+int shim_read_file_f64(const char *path, size_t input_count, double *out, size_t *count) {
+  return guarded([&] {
+    auto r = data::arrays::read_file_as<double>(path, input_count);
+    std::memcpy(out, r.first, sizeof(double) * r.second);
+    *count = r.second;
+    delete[] r.first;
+  });
+}
+
 #define ALP_DECODE(SUF, T, U)                                                                 \
   int shim_decompress_alp_##SUF(const U *packed, size_t n_packed, const uint8_t *bw,         \
                                 const size_t *offs, const U *bases, size_t n_values,         \

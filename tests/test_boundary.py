@@ -60,6 +60,27 @@ def test_shim_and_device_header_build_and_export(built):
         assert hasattr(d, "user_decode_" + k), k
 
 
+def test_shim_read_file_as(built, tmp_path):
+    """data::arrays::read_file_as: whole vectors of the file, repeated when
+    the file is shorter than the count asked for; errors as exceptions."""
+    s = C.CDLL(str(built[0]))
+    vals = np.random.default_rng(1).standard_normal(2500)
+    path = tmp_path / "col.bin"
+    vals.tofile(path)
+    out = np.zeros(8192, np.float64)
+    n = C.c_size_t(0)
+    assert s.shim_read_file_f64(str(path).encode(), C.c_size_t(0), _p(out), C.byref(n)) == 0
+    assert n.value == 2048 and np.array_equal(out[:2048], vals[:2048])
+    assert s.shim_read_file_f64(str(path).encode(), C.c_size_t(7000), _p(out), C.byref(n)) == 0
+    assert n.value == 6144
+    assert np.array_equal(out[:6144], np.resize(vals, 6144))
+    (tmp_path / "bad.bin").write_bytes(b"12345")
+    assert s.shim_read_file_f64(str(tmp_path / "bad.bin").encode(), C.c_size_t(0), _p(out),
+                                C.byref(n)) == 1
+    assert s.shim_read_file_f64(str(tmp_path / "missing.bin").encode(), C.c_size_t(0), _p(out),
+                                C.byref(n)) == 1
+
+
 def _p(a):
     return C.c_void_p(a.ctypes.data) if a.size else C.c_void_p(16)
 
