@@ -15,7 +15,7 @@ def random_ffor(seed: int, n_vecs: int, bits: int, widths, base_max: int | None 
     """Random FastLanes column: per-vector width drawn from `widths`, random
     packed words (every value uniform in [0, 2^w)), random bases."""
     rng = np.random.default_rng(seed)
-    ut = np.uint64 if bits == 64 else np.uint32
+    ut = {8: np.uint8, 16: np.uint16, 32: np.uint32, 64: np.uint64}[bits]
     nl = 1024 // bits
     bw = rng.choice(np.asarray(list(widths)), n_vecs).astype(np.uint8)
     offs = np.zeros(n_vecs, np.uint64)
