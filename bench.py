@@ -385,10 +385,10 @@ def make_alp_columns(scale: float, dev, seed: int = 31):
     * f64 ALP-RD, 2^27 values uniform in [0, 1) with full mantissa, encoded
       by the library's GPU ALP-RD encoder (cut and dictionary per rowgroup of
       100 vectors);
-    * f32 ALP, 2^28 values: integers uniform in [-10^6, 10^6] times
-      FRAC[d] (d uniform per vector in 0..3, factor 0: the value ALP decodes
-      them to), FFOR-packed at the signed minimum by the GPU packer, 1% of
-      positions replaced by random non-NaN 32-bit patterns as exceptions.
+    * f32 ALP, 2^28 values: integers uniform in [-10^6, 10^6] times the
+      float 10^-d (d uniform per vector in 0..3: the values ALP decodes to),
+      1% of positions replaced by random non-NaN 32-bit patterns; encoded by
+      the library's GPU f32 encoder.
     Returns [(name, column, expected values, read bytes, written bytes)]."""
     import torch
     import flsgpu_b200 as F
@@ -432,7 +432,9 @@ def make_alp_columns(scale: float, dev, seed: int = 31):
             + int(rres.n_dictionaries) * 16 + int(rres.n_exceptions) * 4)
     out.append(("alprd_f64", col, vals, rd_b, n * 8))
 
-    # f32 ALP, compressed level with the values ALP decodes to
+    # f32 ALP, value level: integers times the float 10^-d (the values ALP
+    # decodes to), 1% random non-NaN patterns; encoded by the library's GPU
+    # f32 encoder (plain per-vector search)
     n = int(2 ** 28 * scale) // 1024 * 1024
     nv = n // 1024
     ints = torch.randint(-10 ** 6, 10 ** 6 + 1, (n,), dtype=torch.int32, device=dev, generator=g)
@@ -443,20 +445,12 @@ def make_alp_columns(scale: float, dev, seed: int = 31):
     pat = torch.randint(-2 ** 31, 2 ** 31 - 1, (n,), dtype=torch.int32, device=dev, generator=g)
     pat = torch.where(torch.isnan(pat.view(torch.float32)), pat & ~(1 << 30), pat)
     vals.view(torch.int32)[m] = pat[m]
-    counts, eoffs, flat, pos = exc_layout(m, nv)
-    exc = vals[flat].contiguous()
-    fcol = F.ffor_encode(ints, F.BASE_SIGNED_MIN)
-    fac = torch.zeros(nv, dtype=torch.uint8, device=dev)
-    fr = dv.to(torch.uint8)
-    n_exc = int(flat.numel())
-    c = F.ALPColumnC(n, fcol.c, None, None, fac.data_ptr(), fr.data_ptr(), n_exc,
-                     eoffs.data_ptr(), exc.data_ptr(), pos.data_ptr(), counts.data_ptr())
-    keep = {"ffor": fcol, "fac": fac, "fr": fr, "exc": exc, "pos": pos, "counts": counts,
-            "eoffs": eoffs}
-    col = F.DeviceColumn("alp", "f32", n, c, {"_keep": keep}, fcol.n_packed)
-    rd_b = fcol.n_packed * 4 + nv * 25 + n_exc * 6
+    del ints, m, pat, dv
+    enc32 = F.AlpEncoder(seed=3)
+    res = enc32.encode_f32(vals)
+    col = F.encoded_column(res, n, enc32, dtype="f32")
+    rd_b = int(res.n_packed_words) * 4 + nv * 25 + int(res.n_exceptions) * 6
     out.append(("alp_f32", col, vals, rd_b, n * 4))
-    del ints, m, pat
     return out
 
 
