@@ -367,8 +367,9 @@ def run_ffor_sum(args, cols, out, dev):
             "decoded_equivalent_gbs": round(decoded / (ms / 1e3) / 1e9, 1),
             "ms_per_step": round(ms, 3), "steps": n, "columns": len(cols),
             "kernel": "k_column<T, FFOR, S_SUM> (flsgpu_sum_ffor_u32/u64)",
-            "issue_bound_note": "at low widths the unpack-and-add of 2^28 values per column, not "
-                                "the compressed reads, bounds the kernel",
+            "bound_note": "at low widths a column's compressed reads take a few microseconds; "
+                          "the kernel is then bound by each warp's load latency per vector "
+                          "(reads only, nothing else in flight), not by HBM",
             "sum_exact_vs_decoded": exact, "gpu_launches_per_step": launches,
             "clocks": clk.summary()}
 

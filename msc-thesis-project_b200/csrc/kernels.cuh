@@ -597,9 +597,22 @@ __global__ void __launch_bounds__(256, min_blocks<T, VAR>()) k_column(const Kern
     } else {
       // register sinks for integer columns
       if constexpr (SINK == S_SUM) {
-        decode_values<T>(vin, w, t, xf, [&](int idx, T v, auto...) {
-          if (idx < lim) acc_u += (uint64_t)v;
-        });
+        // sum of (u + base): with 64-bit lanes the accumulator wraps as the
+        // values do, so the base enters once per vector (1024 * base); with
+        // 32-bit lanes only when no value of the vector wraps (base + 2^w - 1
+        // < 2^32).  Full vectors take no per-value bound test.
+        const U base = xf.base;
+        const bool once = sizeof(U) == 8 || (uint64_t)base + ((1ull << w) - 1ull) < (1ull << 32);
+        if (lim == VEC && once) {
+          uint64_t sv = 0;
+          decode_values<T, VAR>(vin, w, t, XInt<U>{U(0)},
+                                [&](int, T v, auto...) { sv += (uint64_t)v; });
+          acc_u += sv + (t == 0 ? (uint64_t)base * (uint64_t)VEC : 0ull);
+        } else {
+          decode_values<T, VAR>(vin, w, t, xf, [&](int idx, T v, auto...) {
+            if (idx < lim) acc_u += (uint64_t)v;
+          });
+        }
       } else if constexpr (SINK == S_QUERY) {
         decode_values<T>(vin, w, t, xf, [&](int idx, T v, auto...) { flag |= (idx < lim) && (v == magic); });
       } else if constexpr (SINK == S_COMPUTE) {
@@ -670,11 +683,17 @@ template <typename T, int KIND> flsgpu_status launch_staged(const KernelParams &
 template <typename T, int KIND, int SINK> struct Launch {
   static constexpr bool STAGE = (KIND == K_ALP || KIND == K_ALPX) && SINK != S_STORE;
   static size_t smem() { return STAGE ? (size_t)8 * VEC * sizeof(T) : 0; }
+  // Integer sums hold no decoded values, only the packed words in flight:
+  // their kernel is register-capped for twice the resident warps (wide
+  // 64-bit half-lanes decode in two runs of 16), which doubles the loads
+  // each SM keeps in flight.
+  static constexpr int COL_VAR =
+      (SINK == S_SUM && (KIND == K_BP || KIND == K_FFOR)) ? (VAR_AUTO | VAR_OCC) : VAR_DEFAULT;
   template <int V> static auto kernel() {
     if constexpr (SINK == S_STORE)
       return k_store<T, KIND, VAR_AUTO | V>;
     else
-      return k_column<T, KIND, SINK>;
+      return k_column<T, KIND, SINK, COL_VAR>;
   }
   template <int V> static int blocks_per_sm() {
     static int bps = 0;
