@@ -500,6 +500,59 @@ __global__ void __launch_bounds__(256, min_blocks<T, VAR>()) k_store(const Kerne
   }
 }
 
+// ---- integer sums: the sum of a thread's 32 packed values ------------------
+// A thread's 32 values of width W are the stream of its W words w[0..W-1]
+// (lane t of a 32-bit vector, or half-lane t / 16 of lane t % 16 of a
+// 64-bit one after words_of_half64): value k is stream bits [kW, kW + W).
+// Bit o of word j is therefore bit (32 j + o) mod W of its value, and the
+// sum of the 32 values is sum over j, b of popc(w[j] & M(W, j, b)) << b,
+// where M(W, j, b) marks the bits of word j at value bit b -- W * W
+// popcounts instead of 32 unpacks and adds, fewer instructions up to
+// kPopW.  Up to 26 bits the 32 values sum within 32 bits.
+constexpr int kPopW = 4;
+constexpr int kSum32W = 26;
+
+__host__ __device__ constexpr uint32_t plane_mask(int W, int j, int b) {
+  uint32_t m = 0;
+  for (int o = 0; o < 32; ++o)
+    if ((32 * j + o) % W == b) m |= 1u << o;
+  return m;
+}
+
+template <int W, int J, int B>
+__device__ __forceinline__ uint32_t plane_sum(const uint32_t *w) {
+  if constexpr (J == W) {
+    return 0u;
+  } else if constexpr (B == W) {
+    return plane_sum<W, J + 1, 0>(w);
+  } else {
+    constexpr uint32_t M = plane_mask(W, J, B);
+    return ((uint32_t)__popc(w[J] & M) << B) + plane_sum<W, J, B + 1>(w);
+  }
+}
+
+// Sum of the calling thread's 32 values u (without the base) of a vector
+// of width w <= kSum32W.
+template <typename U>
+__device__ __forceinline__ uint32_t thread_sum_narrow(const U *vin, int w, int t) {
+  uint32_t s = 0;
+  switch_width26(w, [&](auto wc) {
+    constexpr int W = decltype(wc)::value;
+    if constexpr (W > 0) {
+      uint32_t wr[W];
+      if constexpr (sizeof(U) == 4)
+        load_lane32<W>(vin, t, wr);
+      else
+        load_half64<W>(vin, t & 15, t >> 4, wr);
+      if constexpr (W <= kPopW)
+        s = plane_sum<W, 0, 0>(wr);
+      else
+        unpack_lane32<W>(wr, [&](int, uint32_t u) { s += u; });
+    }
+  });
+  return s;
+}
+
 template <typename T, int KIND, int SINK, int VAR = VAR_DEFAULT>
 __global__ void __launch_bounds__(256, min_blocks<T, VAR>()) k_column(const KernelParams p) {
   using U = typename UintOf<T>::U;
@@ -605,8 +658,11 @@ __global__ void __launch_bounds__(256, min_blocks<T, VAR>()) k_column(const Kern
         const bool once = sizeof(U) == 8 || (uint64_t)base + ((1ull << w) - 1ull) < (1ull << 32);
         if (lim == VEC && once) {
           uint64_t sv = 0;
-          decode_values<T, VAR>(vin, w, t, XInt<U>{U(0)},
-                                [&](int, T v, auto...) { sv += (uint64_t)v; });
+          if (w <= kSum32W)
+            sv = thread_sum_narrow<U>(vin, w, t);
+          else
+            decode_values<T, VAR>(vin, w, t, XInt<U>{U(0)},
+                                  [&](int, T v, auto...) { sv += (uint64_t)v; });
           acc_u += sv + (t == 0 ? (uint64_t)base * (uint64_t)VEC : 0ull);
         } else {
           decode_values<T, VAR>(vin, w, t, xf, [&](int idx, T v, auto...) {

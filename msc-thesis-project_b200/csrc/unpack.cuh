@@ -226,6 +226,14 @@ __device__ __forceinline__ bool dispatch_width(int w, F &&f) {
   FLSB_CASE(58) FLSB_CASE(59) FLSB_CASE(60) FLSB_CASE(61) FLSB_CASE(62)            \
   FLSB_CASE(63) FLSB_CASE(64)
 
+template <class F> __device__ __forceinline__ bool switch_width26(int w, F &&f) {
+  switch (w) {
+    FLSB_CASES_0_15
+    FLSB_CASE(16) FLSB_CASE(17) FLSB_CASE(18) FLSB_CASE(19) FLSB_CASE(20) FLSB_CASE(21)
+    FLSB_CASE(22) FLSB_CASE(23) FLSB_CASE(24) FLSB_CASE(25) FLSB_CASE(26)
+    default: return false;
+  }
+}
 template <class F> __device__ __forceinline__ bool switch_width16(int w, F &&f) {
   switch (w) { FLSB_CASES_0_15 FLSB_CASE(16) default: return false; }
 }

@@ -185,3 +185,43 @@ def test_staged_decode_every_width_and_unaligned_vectors(cuda, bp):
     status = torch.zeros(1, dtype=torch.int32, device=cuda)
     F.decompress(d, o=F.opts(variant=F.VARIANT_STAGED, d_status=status))
     assert int(status.item()) == 0
+
+
+@pytest.mark.parametrize("bits", [32, 64])
+def test_fused_sum_groups_and_edges(cuda, bits):
+    """The integer sum adds each full vector's base once (1024 * base) when
+    that is exact and sums value by value otherwise: exact (mod 2^64)
+    against the oracle on long runs of one narrow width, on narrow and wide
+    widths mixed, on u32 bases whose values wrap past 2^32 (every vector,
+    and every third vector), on ragged tails and on a single partial
+    vector; a bad width among narrow vectors is flagged and adds nothing."""
+    import torch
+    ut = np.uint64 if bits == 64 else np.uint32
+
+    def ref(c, n_values=None):
+        want = B.decode_ffor(c["packed"], c["bit_widths"], c["vector_offsets"], c["bases"], bits)
+        return int(want[:n_values].astype(np.uint64).sum(dtype=np.uint64))
+
+    cases = [([3], 9000, None), ([1, 2, 9, 8, 30, 0], 9000, None), (range(9), 9001, 9001 * 1024 - 5),
+             ([5], 7, 7 * 1024 - 1), ([0, 1], 1, 1)]
+    for i, (widths, n_vecs, n_values) in enumerate(cases):
+        c = colgen.random_ffor(1700 + i + bits, n_vecs, bits, widths, n_values=n_values)
+        if i == 0 and bits == 32:
+            c["bases"][:] = np.uint32(2 ** 32 - 3)  # every vector's values wrap
+        s = int(F.sum_(_col(c, cuda)).cpu().numpy().view(np.uint64)[0])
+        assert s == ref(c, c["n_values"]), (bits, i)
+    # bases near the top of the u32 range on some vectors only
+    if bits == 32:
+        c = colgen.random_ffor(1790, 5000, 32, [4, 7])
+        c["bases"][::3] = np.uint32(2 ** 32 - 1)
+        assert int(F.sum_(_col(c, cuda)).cpu().numpy().view(np.uint64)[0]) == ref(c)
+    # a bad width among narrow vectors: flagged, the rest summed
+    c = colgen.random_ffor(1791 + bits, 6000, bits, [2])
+    want = B.decode_ffor(c["packed"], c["bit_widths"], c["vector_offsets"], c["bases"], bits)
+    keep = np.ones(6000 * 1024, bool)
+    keep[2500 * 1024:2501 * 1024] = False
+    c["bit_widths"][2500] = bits + 1
+    status = torch.zeros(1, dtype=torch.int32, device=cuda)
+    s = int(F.sum_(_col(c, cuda), o=F.opts(d_status=status)).cpu().numpy().view(np.uint64)[0])
+    assert int(status.item()) & F.BAD_BIT_WIDTH
+    assert s == int(want[keep].astype(np.uint64).sum(dtype=np.uint64))
