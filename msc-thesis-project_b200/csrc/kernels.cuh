@@ -203,6 +203,7 @@ constexpr int VAR_PAIR = 64;     // decode two same-width vectors per warp step 
 constexpr int VAR_NOPAIR = 128;  // kernel variant: never pair
 constexpr int VAR_MINB4 = 256;   // kernel variant: 32-bit lanes capped for four blocks per SM
 constexpr int VAR_OCC = 512;     // kernel variant: registers capped for twice the resident blocks
+constexpr int VAR_MINB3 = 1024;  // kernel variant: registers capped for three resident blocks
 constexpr int VAR_DEFAULT = VAR_AUTO;
 
 // Policy bits in force for width W under kernel variant VAR.
@@ -343,7 +344,7 @@ template <typename T, int T_VAR> __device__ __forceinline__ void store_out(T *p,
 // keeping every packed word of the widest cases in registers.
 template <typename T, int VAR> constexpr int min_blocks() {
   constexpr int base = sizeof(T) == 4 ? 2 : 1;
-  return (VAR & VAR_MINB4) ? 4 : (VAR & VAR_MINB2) ? 2 : (VAR & VAR_OCC) ? 2 * base : base;
+  return (VAR & VAR_MINB4) ? 4 : (VAR & VAR_MINB3) ? 3 : (VAR & VAR_MINB2) ? 2 : (VAR & VAR_OCC) ? 2 * base : base;
 }
 
 __device__ __forceinline__ bool prefetch_width(const KernelParams &p, int w) {
@@ -744,7 +745,9 @@ template <typename T, int KIND, int SINK> struct Launch {
   // 64-bit half-lanes decode in two runs of 16), which doubles the loads
   // each SM keeps in flight.
   static constexpr int COL_VAR =
-      (SINK == S_SUM && (KIND == K_BP || KIND == K_FFOR)) ? (VAR_AUTO | VAR_OCC) : VAR_DEFAULT;
+      (SINK == S_SUM && (KIND == K_BP || KIND == K_FFOR))
+          ? (VAR_AUTO | VAR_OCC | (sizeof(T) == 8 ? VAR_MINB3 : 0))
+          : VAR_DEFAULT;
   template <int V> static auto kernel() {
     if constexpr (SINK == S_STORE)
       return k_store<T, KIND, VAR_AUTO | V>;
