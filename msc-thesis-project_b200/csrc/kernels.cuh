@@ -582,8 +582,10 @@ __global__ void __launch_bounds__(256, min_blocks<T, VAR>()) k_column(const Kern
     const Meta<T> cur = meta;
     if (vi + nw < c.n_vecs) {
       meta = load_meta<T, KIND>(c, vi + nw);
-      if (meta.w <= (int)(sizeof(U) * 8) && prefetch_width(p, meta.w))
-        prefetch_packed(reinterpret_cast<const U *>(c.packed) + meta.off, meta.w, t);
+      bool pf = meta.w <= (int)(sizeof(U) * 8) && prefetch_width(p, meta.w);
+      if constexpr (SINK == S_QUERY && !IS_ALP)  // not for a vector the range test skips
+        pf = pf && (meta.w == (int)(sizeof(U) * 8) || (((U)magic - meta.base) >> meta.w) == 0);
+      if (pf) prefetch_packed(reinterpret_cast<const U *>(c.packed) + meta.off, meta.w, t);
     }
     if (!setup_from_meta<T, KIND>(c, p.d_status, cur, t, vin, w, xf)) {
       // a rejected vector (status flag raised) adds +0.0: its slot of the
@@ -671,7 +673,18 @@ __global__ void __launch_bounds__(256, min_blocks<T, VAR>()) k_column(const Kern
           });
         }
       } else if constexpr (SINK == S_QUERY) {
-        decode_values<T>(vin, w, t, xf, [&](int idx, T v, auto...) { flag |= (idx < lim) && (v == magic); });
+        // a vector of width w holds (u + base) mod 2^bits with u < 2^w: it
+        // can hold the magic value only if u = (magic - base) mod 2^bits is
+        // below 2^w, so other vectors are decided on their metadata alone
+        const U target = (U)magic - xf.base;
+        if (w < (int)(sizeof(U) * 8) && (target >> w) != 0) continue;
+        if (lim == VEC) {
+          decode_values<T, VAR>(vin, w, t, XInt<U>{U(0)},
+                                [&](int, T v, auto...) { flag |= v == target; });
+        } else {
+          decode_values<T, VAR>(vin, w, t, XInt<U>{U(0)},
+                                [&](int idx, T v, auto...) { flag |= (idx < lim) && (v == target); });
+        }
       } else if constexpr (SINK == S_COMPUTE) {
         const T zero = (T)p.runtime_zero;
         const uint32_t nrep = p.n_rep;
@@ -740,13 +753,13 @@ template <typename T, int KIND> flsgpu_status launch_staged(const KernelParams &
 template <typename T, int KIND, int SINK> struct Launch {
   static constexpr bool STAGE = (KIND == K_ALP || KIND == K_ALPX) && SINK != S_STORE;
   static size_t smem() { return STAGE ? (size_t)8 * VEC * sizeof(T) : 0; }
-  // Integer sums hold no decoded values, only the packed words in flight:
-  // their kernel is register-capped for twice the resident warps (wide
-  // 64-bit half-lanes decode in two runs of 16), which doubles the loads
+  // Integer sums and scans hold no decoded values, only the packed words in
+  // flight: their kernel is register-capped for more resident warps (wide
+  // 64-bit half-lanes decode in two runs of 16), which multiplies the loads
   // each SM keeps in flight.
   static constexpr int COL_VAR =
-      (SINK == S_SUM && (KIND == K_BP || KIND == K_FFOR))
-          ? (VAR_AUTO | VAR_OCC | (sizeof(T) == 8 ? VAR_MINB3 : 0))
+      ((SINK == S_SUM || SINK == S_QUERY) && (KIND == K_BP || KIND == K_FFOR))
+          ? (VAR_AUTO | VAR_OCC | (sizeof(T) == 8 && SINK == S_SUM ? VAR_MINB3 : 0))
           : VAR_DEFAULT;
   template <int V> static auto kernel() {
     if constexpr (SINK == S_STORE)

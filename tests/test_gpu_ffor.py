@@ -225,3 +225,36 @@ def test_fused_sum_groups_and_edges(cuda, bits):
     s = int(F.sum_(_col(c, cuda), o=F.opts(d_status=status)).cpu().numpy().view(np.uint64)[0])
     assert int(status.item()) & F.BAD_BIT_WIDTH
     assert s == int(want[keep].astype(np.uint64).sum(dtype=np.uint64))
+
+
+@pytest.mark.parametrize("bits", [32, 64])
+def test_query_range_test_edges(cuda, bits):
+    """The integer scan decides a vector on its metadata when the magic
+    value lies outside [base, base + 2^w) (mod 2^bits): found exactly where
+    the oracle's decode holds the value -- a vector's base (u = 0), its top
+    value (u = 2^w - 1), values of vectors whose range wraps past 2^bits,
+    width-0 vectors (only the base), full-width vectors (no test) -- and not
+    found for values just outside a range or present only past n_values in
+    the last, partial vector."""
+    ut = np.uint64 if bits == 64 else np.uint32
+    top = 2 ** bits
+    rng = np.random.default_rng(bits)
+    for widths in ([0, 3], [1, 7, bits], [5]):
+        n_vecs = 64
+        n_values = n_vecs * 1024 - 300
+        c = colgen.random_ffor(2100 + bits + len(widths), n_vecs, bits, widths, n_values=n_values)
+        # some bases near the top of the range, so that their values wrap
+        c["bases"][::5] = ut(top - 3)
+        vals = B.decode_ffor(c["packed"], c["bit_widths"], c["vector_offsets"], c["bases"], bits)
+        inside = set(int(x) for x in vals[:n_values])
+        col = _col(c, cuda)
+        cands = set()
+        for v in rng.choice(n_vecs - 1, 12, replace=False):
+            w, base = int(c["bit_widths"][v]), int(c["bases"][v])
+            cands |= {base, (base + 2 ** min(w, bits) - 1) % top, (base + 2 ** min(w, bits)) % top,
+                      (base - 1) % top}
+        cands |= set(int(x) for x in vals[n_values:n_vecs * 1024][:5])  # past n_values
+        cands |= {0, top - 1, int(vals[n_values - 1])}
+        for m in sorted(cands):
+            got = int(F.query(col, m).item())
+            assert got == (m in inside), (widths, m)
