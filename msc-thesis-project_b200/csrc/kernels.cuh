@@ -1015,6 +1015,16 @@ __global__ void __launch_bounds__(256) k_multi(const MultiParams mp) {
         all = false;
         continue;
       }
+      [[maybe_unused]] U target = 0;
+      if constexpr (!IS_ALP) {
+        // the vector holds (u + base) mod 2^bits with u < 2^w: no lane can
+        // equal the value throughout unless (value - base) mod 2^bits < 2^w
+        target = (U)value - xf.base;
+        if (w < (int)(sizeof(U) * 8) && (target >> w) != 0) all = false;
+      }
+      // once no lane of the warp can qualify, the vector's remaining columns
+      // are only validated (their metadata checks still raise the status)
+      if (!__any_sync(0xffffffffu, all && (!IS_ALP || t < NL))) continue;
       const size_t rem = c.n_values - vi * VEC;
       const int lim = rem < (size_t)VEC ? (int)rem : VEC;
       if constexpr (IS_ALP) {
@@ -1029,7 +1039,8 @@ __global__ void __launch_bounds__(256) k_multi(const MultiParams mp) {
           }
         __syncwarp();
       } else {
-        decode_values<T>(vin, w, t, xf, [&](int idx, T v, auto...) { all &= (idx >= lim) || (v == value); });
+        decode_values<T>(vin, w, t, XInt<U>{U(0)},
+                         [&](int idx, T v, auto...) { all &= (idx >= lim) || (v == target); });
       }
     }
     if constexpr (IS_ALP) {

@@ -258,3 +258,55 @@ def test_query_range_test_edges(cuda, bits):
         for m in sorted(cands):
             got = int(F.query(col, m).item())
             assert got == (m in inside), (widths, m)
+
+
+@pytest.mark.parametrize("bits", [32, 64])
+def test_multi_column_range_test_and_skips(cuda, bits):
+    """The multi-column scan decides a vector of a column on its metadata
+    when the value lies outside the vector's range and stops decoding a
+    vector's columns once no lane can qualify: same answers as the oracle's
+    decode, per lane, on columns whose vectors mix width-0 runs of the
+    value, narrow widths around it and wrapping bases; a corrupt width in a
+    later column of a vector that already failed is still flagged."""
+    import torch
+    ut = np.uint64 if bits == 64 else np.uint32
+    top = 2 ** bits
+    n_vecs = 48
+    nl = 1024 // bits
+    rng = np.random.default_rng(5 + bits)
+
+    def column(seed, widths, base_of):
+        c = colgen.random_ffor(seed, n_vecs, bits, [0])
+        c["bit_widths"][:] = widths
+        c["vector_offsets"][:] = np.concatenate(
+            [[0], np.cumsum(c["bit_widths"].astype(np.uint64) * nl)[:-1]])
+        n = int(c["bit_widths"].astype(np.int64).sum()) * nl
+        c["packed"] = rng.integers(0, 2 ** 63, max(n, 1), dtype=np.uint64).astype(ut)[:n]
+        c["bases"][:] = [ut(base_of(v) % top) for v in range(n_vecs)]
+        return c
+
+    def lanes_equal(cols, value):
+        lanes = 1024 // bits  # FastLanes lanes; lane l holds values l + lanes * k
+        ok = False
+        vals = [B.decode_ffor(c["packed"], c["bit_widths"], c["vector_offsets"], c["bases"], bits)
+                .reshape(n_vecs, 1024 // lanes, lanes) for c in cols]
+        for v in range(n_vecs):
+            every = np.ones(lanes, bool)
+            for x in vals:
+                every &= np.all(x[v] == ut(value % top), axis=0)
+            ok |= bool(every.any())
+        return ok
+
+    value = 7
+    widths_a = np.where(np.arange(n_vecs) % 3 == 0, 0, np.where(np.arange(n_vecs) % 3 == 1, 2, 5))
+    cols = [column(2200 + bits, widths_a, lambda v: 7 if v % 3 == 0 else 6),
+            column(2201 + bits, np.where(np.arange(n_vecs) % 2 == 0, 0, 3), lambda v: 7 if v % 4 else top - 2),
+            column(2202 + bits, np.zeros(n_vecs, np.int64), lambda v: 7 if v != 9 else 8)]
+    d = [_col(c, cuda) for c in cols]
+    for m in (value, 6, 8, top - 2, 0):
+        assert int(F.query_multi_column(d, m).item()) == int(lanes_equal(cols, m)), m
+    # a corrupt width in the last column of vectors that fail on column 0
+    cols[2]["bit_widths"][1] = bits + 1
+    status = torch.zeros(1, dtype=torch.int32, device=cuda)
+    F.query_multi_column([_col(c, cuda) for c in cols], 12345, o=F.opts(d_status=status))
+    assert int(status.item()) & F.BAD_BIT_WIDTH
