@@ -831,8 +831,12 @@ def run_learned(args, dev):
         exact_plain = bool(torch.equal(dec.view(torch.int64), evals.view(torch.int64)))
         ms_learned = ev_time(lambda: res.__setitem__("learned", enc.encode_hybrid(evals, 1)))
         learned = res["learned"]
-        dec = F.decompress(F.hybrid_column(learned, evals.numel(), enc))
+        hcol = F.hybrid_column(learned, evals.numel(), enc)
+        dec = F.decompress(hcol)
         exact = bool(torch.equal(dec.view(torch.int64), evals.view(torch.int64))) and exact_plain
+        # decode of the learned hybrid column (before the encoder's next
+        # encode reuses its workspace)
+        ms_hdec = ev_time(lambda: F.decompress(hcol, out=dec))
         # the same two encoders writing ALP-only columns (ALP-RD vectors kept
         # on their best ALP pair), as the reference's ALPColumn requires
         ms_plain_a = ev_time(lambda: res.__setitem__("plain_a", enc.encode(evals, 0)))
@@ -861,7 +865,7 @@ def run_learned(args, dev):
                 ms_propose=ms_propose, in_bytes=in_bytes, plain_bytes=plain_bytes,
                 learned_bytes=learned.compressed_bytes, fallback=int(learned.n_fallback),
                 n_rd=int(learned.n_rd_vectors), plain_rd=plain_rd, alp_only=alp_only,
-                n_vecs=evals.numel() // 1024, exact=exact,
+                n_vecs=evals.numel() // 1024, exact=exact, ms_hdec=ms_hdec,
                 loss=(l0, l1), train_s=train_s, clocks=clk.summary(),
                 ref_gbs=sample.nbytes / ref_s / 1e9 if ref_col is not None else None,
                 ref_ratio=sample.nbytes / ref_col["compressed_bytes"] if ref_col is not None else None)
@@ -1237,7 +1241,10 @@ def learned_block(args, dev, world) -> dict:
                     "ratio": round(r["in_bytes"] / r["learned_bytes"], 4),
                     "fallback_vectors": r["fallback"], "rd_vectors": r["n_rd"],
                     "proposal_ms": round(r["ms_propose"], 3),
-                    "decode_bit_exact": r["exact"]},
+                    "decode_bit_exact": r["exact"],
+                    "decode_gbs": round((r["learned_bytes"] + r["in_bytes"]) / (r["ms_hdec"] / 1e3)
+                                        / 1e9, 1),
+                    "decode_kernel": "k_hybrid<double> (flsgpu_decompress_alphybrid_f64)"},
         "plain": {"encode_gbs": round(gbs_p, 1), "ms": round(r["ms_plain"], 3),
                   "ratio": round(r["in_bytes"] / r["plain_bytes"], 4),
                   "rd_vectors": r["plain_rd"], "search_ms": round(r["ms_search"], 3)},

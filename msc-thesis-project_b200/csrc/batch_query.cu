@@ -293,13 +293,8 @@ __global__ void __launch_bounds__(256, 2)
         __syncwarp();
         bool bad = (uint32_t)t < ecnt && p0 >= VEC;
         if (p0 < VEC) sa[p0] = e0;
-        for (uint32_t i = t + 32; i < ecnt; i += 32) {
-          const uint32_t ps = pe.a.pos[ma.eo + i];
-          if (ps < VEC)
-            sa[ps] = exc[ma.eo + i];
-          else
-            bad = true;
-        }
+        bad |= patch_batched<double>(pe.a.pos + ma.eo, exc + ma.eo, 32, ecnt, t,
+                                     [&](uint32_t ps, double e) { sa[ps] = e; });
         if (__any_sync(0xffffffffu, bad) && t == 0) flag_status(d_status, FLSGPU_BAD_EXCEPTION);
         __syncwarp();
 #pragma unroll 8

@@ -302,6 +302,38 @@ __device__ __forceinline__ void decode_pair(const typename UintOf<T>::U *va,
   }
 }
 
+// Writes exceptions [from, cnt) of a vector (positions pos[i], values
+// exc[i], both already offset to the vector's first exception) through
+// write(position, value), four rounds of 32 at a time: every load of a
+// batch is issued before its stores, so a vector with many exceptions waits
+// one load latency per 128 of them instead of one per 32 (the stores may
+// alias the loads as far as the compiler knows, so it cannot reorder them
+// itself).  Returns true when a position was out of range (not written).
+template <typename T, class Write>
+__device__ __forceinline__ bool patch_batched(const uint16_t *pos, const T *exc, uint32_t from,
+                                              uint32_t cnt, int t, Write &&write) {
+  bool bad = false;
+  for (uint32_t i0 = from; i0 < cnt; i0 += 128) {
+    uint32_t ps[4];
+    T ev[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const uint32_t i = i0 + 32u * u + (uint32_t)t;
+      ps[u] = i < cnt ? (uint32_t)pos[i] : 0xFFFFFFFFu;
+      ev[u] = i < cnt ? exc[i] : T(0);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      if (ps[u] == 0xFFFFFFFFu) continue;
+      if (ps[u] < (uint32_t)VEC)
+        write(ps[u], ev[u]);
+      else
+        bad = true;
+    }
+  }
+  return bad;
+}
+
 // Exceptions of vector vi (decoder::patch_exceptions, src/alp/decoder.hpp:
 // 137-145): count = counts[vi] (ALPColumn) or the u16 sum of the per-lane
 // counts (ALPExtendedColumn, as alp::decode reconstructs it,
@@ -321,14 +353,7 @@ __device__ __forceinline__ void patch_vector(const ColumnParams &c, uint32_t *d_
   }
   const size_t eo = c.exc_offs[vi];
   const T *exc = reinterpret_cast<const T *>(c.exc);
-  bool bad = false;
-  for (uint32_t i = t; i < cnt; i += 32) {
-    const uint32_t ps = c.pos[eo + i];
-    if (ps < VEC)
-      write(ps, exc[eo + i]);
-    else
-      bad = true;
-  }
+  const bool bad = patch_batched<T>(c.pos + eo, exc + eo, 0, cnt, t, write);
   if (__any_sync(0xffffffffu, bad) && t == 0) flag_status(d_status, FLSGPU_BAD_EXCEPTION);
 }
 
@@ -401,14 +426,9 @@ __device__ __forceinline__ void store_one(const KernelParams &p, size_t vi, cons
       bool bad = (uint32_t)t < ecnt && p0 >= VEC;
       if ((int)p0 < lim) out[p0] = e0;
       const T *exc = reinterpret_cast<const T *>(c.exc);
-      for (uint32_t i = t + 32; i < ecnt; i += 32) {
-        const uint32_t ps = c.pos[m.eo + i];
-        if (ps < VEC) {
-          if ((int)ps < lim) out[ps] = exc[m.eo + i];
-        } else {
-          bad = true;
-        }
-      }
+      bad |= patch_batched<T>(c.pos + m.eo, exc + m.eo, 32, ecnt, t, [&](uint32_t ps, T e) {
+        if ((int)ps < lim) out[ps] = e;
+      });
       if (__any_sync(0xffffffffu, bad) && t == 0) flag_status(p.d_status, FLSGPU_BAD_EXCEPTION);
       return;
     }

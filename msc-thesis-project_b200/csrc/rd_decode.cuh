@@ -124,13 +124,8 @@ __device__ __forceinline__ void rd_decode_vector(const RDParams &p, size_t vi, c
     __syncwarp();
     bool bad = (uint32_t)t < m.cnt && p0 >= VEC;
     if (p0 < VEC) sl[p0] = e0;
-    for (uint32_t i = t + 32; i < m.cnt; i += 32) {
-      const uint32_t ps = p.pos[m.eo + i];
-      if (ps < VEC)
-        sl[ps] = p.exc[m.eo + i];
-      else
-        bad = true;
-    }
+    bad |= patch_batched<uint16_t>(p.pos + m.eo, p.exc + m.eo, 32, m.cnt, t,
+                                   [&](uint32_t ps, uint16_t e) { sl[ps] = e; });
     if (__any_sync(0xffffffffu, bad) && t == 0 && p.d_status)
       atomicOr(p.d_status, FLSGPU_BAD_EXCEPTION);
     __syncwarp();

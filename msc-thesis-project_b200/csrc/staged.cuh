@@ -173,14 +173,9 @@ __device__ __forceinline__ void store_one_staged(const KernelParams &p, size_t v
       bool bad = (uint32_t)t < ecnt && p0 >= VEC;
       if ((int)p0 < lim) out[p0] = e0;
       const T *exc = reinterpret_cast<const T *>(c.exc);
-      for (uint32_t i = t + 32; i < ecnt; i += 32) {
-        const uint32_t ps = c.pos[m.eo + i];
-        if (ps < VEC) {
-          if ((int)ps < lim) out[ps] = exc[m.eo + i];
-        } else {
-          bad = true;
-        }
-      }
+      bad |= patch_batched<T>(c.pos + m.eo, exc + m.eo, 32, ecnt, t, [&](uint32_t ps, T e) {
+        if ((int)ps < lim) out[ps] = e;
+      });
       if (__any_sync(0xffffffffu, bad) && t == 0) flag_status(p.d_status, FLSGPU_BAD_EXCEPTION);
     } else if (c.patch) {
       __syncwarp();
